@@ -1,0 +1,342 @@
+// extern "C" boundary (include/bsz.h).  Exceptions never cross it: each
+// entry point catches, stores the message for bsz_last_error() and returns a
+// status.
+#include "../../include/bsz.h"
+
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "device.h"
+#include "engine.h"
+#include "frontend.h"
+#include "io.h"
+
+struct bsz_ctx {
+  std::unique_ptr<bsz::Device> dev;
+};
+
+struct bsz_program {
+  bsz_ctx* ctx;
+  std::unique_ptr<bsz::Program> prog;
+};
+
+struct bsz_run {
+  bsz_program* prog;
+  int64_t bitlength;
+  int mode;
+  std::unique_ptr<bsz::Executor> ex;
+  std::vector<std::pair<int, int64_t>> params;
+  bool done = false;
+};
+
+namespace {
+
+thread_local std::string g_err;
+thread_local std::string g_json;
+
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+  } catch (...) {
+    g_err = "unknown error";
+  }
+  return 1;
+}
+
+int64_t words_of(int64_t bitlength) { return bitlength > 0 ? (bitlength + 63) / 64 : 1; }
+
+bsz::Executor& executor(bsz_run* r) {
+  if (!r->ex) {
+    bsz::ExecOptions o;
+    o.mode = r->mode == BSZ_MODE_FUSED ? bsz::ExecMode::Fused : bsz::ExecMode::Plain;
+    r->ex = std::make_unique<bsz::Executor>(*r->prog->ctx->dev, *r->prog->prog, r->bitlength, o);
+  }
+  return *r->ex;
+}
+
+int name_id(bsz_run* r, const char* name) {
+  int id = r->prog->prog->find(name ? name : "");
+  if (id < 0) throw std::invalid_argument(std::string("unknown name: ") + (name ? name : "(null)"));
+  return id;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bsz_version(void) { return "bitstreamzoo_b200 0.1 (sm_100a)"; }
+const char* bsz_last_error(void) { return g_err.c_str(); }
+
+bsz_ctx* bsz_create(int device) {
+  bsz_ctx* c = nullptr;
+  if (guard([&] {
+        auto ctx = std::make_unique<bsz_ctx>();
+        ctx->dev = std::make_unique<bsz::Device>(device);
+        c = ctx.release();
+      }))
+    return nullptr;
+  return c;
+}
+
+void bsz_destroy(bsz_ctx* ctx) { delete ctx; }
+
+void* bsz_stream(bsz_ctx* ctx) { return ctx ? static_cast<void*>(ctx->dev->stream()) : nullptr; }
+
+int bsz_sync(bsz_ctx* ctx) {
+  return guard([&] {
+    ctx->dev->sync();
+    if (uint32_t e = ctx->dev->take_error())
+      throw bsz::RuntimeError("device error word " + std::to_string(e));
+  });
+}
+
+bsz_program* bsz_compile(bsz_ctx* ctx, const char* source, size_t len) {
+  bsz_program* p = nullptr;
+  if (guard([&] {
+        auto prog = std::make_unique<bsz_program>();
+        prog->ctx = ctx;
+        prog->prog = bsz::parse_program(std::string(source, len));
+        p = prog.release();
+      }))
+    return nullptr;
+  return p;
+}
+
+void bsz_program_free(bsz_program* prog) { delete prog; }
+
+int64_t bsz_static_ops(bsz_program* prog, const char* const* names, const int64_t* values, int n) {
+  std::unordered_map<std::string, int64_t> params;
+  for (int i = 0; i < n; ++i) params[names[i]] = values[i];
+  return bsz::count_static_ops(*prog->prog, params);
+}
+
+bsz_run* bsz_run_create(bsz_program* prog, int64_t bitlength, int mode) {
+  bsz_run* r = nullptr;
+  if (guard([&] {
+        auto run = std::make_unique<bsz_run>();
+        run->prog = prog;
+        run->bitlength = bitlength;
+        run->mode = mode;
+        executor(run.get());
+        r = run.release();
+      }))
+    return nullptr;
+  return r;
+}
+
+void bsz_run_free(bsz_run* run) { delete run; }
+
+int bsz_set_param(bsz_run* run, const char* name, int64_t value) {
+  return guard([&] {
+    int id = run->prog->prog->find(name);
+    if (id >= 0) executor(run).set_param(id, value);
+  });
+}
+
+int bsz_bind_input(bsz_run* run, const char* name, int64_t index, const uint64_t* words,
+                   uint64_t n_words, int tail, int on_device) {
+  return guard([&] {
+    bsz::Device& dev = *run->prog->ctx->dev;
+    const int id = name_id(run, name);
+    const int64_t nw = words_of(run->bitlength);
+    bsz::BufRef b = dev.alloc_stream(nw);
+    const int64_t have = std::min<int64_t>(static_cast<int64_t>(n_words), nw);
+    if (have > 0)
+      BSZ_CUDA(cudaMemcpyAsync(b->p, words, have * 8,
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                               dev.stream()));
+    if (have < nw) {
+      uint64_t fill = tail ? ~uint64_t(0) : 0;
+      bsz::launch_fill(dev, b->p + have, nw - have, fill, fill);
+    }
+    // Host inputs: check the bits at and above the bitlength.  Device inputs
+    // are treated as possibly dirty there (the executor then keeps them).
+    bool clean = false;
+    if (!on_device && !tail && run->bitlength > 0) {
+      clean = true;
+      const int64_t lw = words_of(run->bitlength);
+      if (have >= lw && (words[lw - 1] & ~bsz::mask_for_bits(run->bitlength))) clean = false;
+    }
+    if (index < 0) executor(run).bind_input(id, b, tail ? 1 : 0, clean);
+    else executor(run).bind_input_array(id, index, b, tail ? 1 : 0, clean);
+  });
+}
+
+int bsz_bind_broadcast(bsz_run* run, const char* name, const uint8_t* ones, int64_t count) {
+  return guard([&] {
+    std::vector<uint8_t> v(ones, ones + count);
+    for (auto& x : v) x = x ? 1 : 0;
+    executor(run).bind_broadcast(name_id(run, name), v);
+  });
+}
+
+int bsz_execute(bsz_run* run, bsz_stats* stats) {
+  return guard([&] {
+    if (run->done) throw bsz::RuntimeError("bsz_execute: run already executed");
+    bsz::Device& dev = *run->prog->ctx->dev;
+    bsz::Executor& ex = executor(run);
+    const int64_t l0 = dev.n_launches;
+    cudaEvent_t e0, e1;
+    BSZ_CUDA(cudaEventCreate(&e0));
+    BSZ_CUDA(cudaEventCreate(&e1));
+    BSZ_CUDA(cudaEventRecord(e0, dev.stream()));
+    ex.run();
+    BSZ_CUDA(cudaEventRecord(e1, dev.stream()));
+    BSZ_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    run->done = true;
+    if (stats) {
+      stats->op_count = ex.op_count;
+      stats->n_kernel_launches = dev.n_launches - l0;
+      stats->n_mallocs = dev.n_mallocs;
+      stats->n_segments = ex.n_segments;
+      stats->n_syncs = ex.n_syncs;
+      stats->peak_bytes = dev.bytes_peak;
+      stats->max_live = ex.max_live_buffers;
+      stats->kernel_ms = ms;
+      stats->compile_ms = ex.compile_ms;
+    }
+  });
+}
+
+static bsz::BufRef find_stream(bsz_run* run, const char* name, int64_t index) {
+  bsz::Executor& ex = executor(run);
+  int id = name_id(run, name);
+  bsz::BufRef b = index < 0 ? ex.stream_value(id) : ex.array_value(id, index);
+  if (!b || (index >= 0 && !ex.has_array(id)) || (index < 0 && !ex.has_stream(id)))
+    throw std::invalid_argument(std::string("no such output: ") + name);
+  return b;
+}
+
+int bsz_get_stream(bsz_run* run, const char* name, int64_t index, uint64_t* host, uint64_t n_words) {
+  return guard([&] {
+    bsz::Device& dev = *run->prog->ctx->dev;
+    bsz::BufRef b = find_stream(run, name, index);
+    const int64_t nw = words_of(run->bitlength);
+    const int64_t n = std::min<int64_t>(nw, static_cast<int64_t>(n_words));
+    BSZ_CUDA(cudaMemcpyAsync(host, b->p, n * 8, cudaMemcpyDeviceToHost, dev.stream()));
+    dev.sync();
+    if (n == nw && run->bitlength > 0) host[nw - 1] &= bsz::mask_for_bits(run->bitlength);
+  });
+}
+
+int bsz_get_stream_device(bsz_run* run, const char* name, int64_t index, const uint64_t** dptr) {
+  return guard([&] { *dptr = find_stream(run, name, index)->p; });
+}
+
+int bsz_get_int(bsz_run* run, const char* name, int64_t* value) {
+  return guard([&] {
+    if (!executor(run).int_value(name_id(run, name), value))
+      throw std::invalid_argument(std::string("no such int: ") + name);
+  });
+}
+
+int64_t bsz_array_indices(bsz_run* run, const char* name, int64_t* indices, int64_t cap) {
+  int64_t count = -1;
+  guard([&] {
+    int id = name_id(run, name);
+    if (!executor(run).has_array(id)) return;
+    auto idx = executor(run).array_indices(id);
+    count = static_cast<int64_t>(idx.size());
+    for (int64_t i = 0; i < count && i < cap; ++i) indices[i] = idx[i];
+  });
+  return count;
+}
+
+const char* bsz_run_case_json(bsz_ctx* ctx, const char* source, const char* bsdata_path,
+                              const char* json_input, int flags) {
+  g_json.clear();
+  int rc = guard([&] {
+    auto t0 = std::chrono::high_resolution_clock::now();
+    auto prog = bsz::parse_program(source);
+    double parse_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::high_resolution_clock::now() - t0).count();
+    std::vector<bsz::CaseInput> cases;
+    if (bsdata_path) cases = bsz::read_bsdata(bsdata_path);
+    else cases.push_back(bsz::parse_json_case(json_input ? json_input : "{}"));
+    bsz::DriverOptions o;
+    o.warmup = flags & 1;
+    o.mode = (flags & 2) ? 1 : 0;
+    if (cases.size() == 1) {
+      g_json = bsz::run_case_json(*ctx->dev, *prog, cases[0], o, parse_ms);
+    } else {
+      g_json = "[";
+      for (size_t i = 0; i < cases.size(); ++i) {
+        std::string one = bsz::run_case_json(*ctx->dev, *prog, cases[i], o, parse_ms);
+        one.pop_back();
+        one += ",\"name\":" + bsz::json_quote(cases[i].name) + "}";
+        if (i) g_json += ",";
+        g_json += one;
+      }
+      g_json += "]";
+    }
+  });
+  return rc ? nullptr : g_json.c_str();
+}
+
+// ---- per-op data plane --------------------------------------------------
+int bsz_op_not(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, uint64_t n, int64_t bitlength) {
+  return guard([&] { bsz::launch_not(*ctx->dev, dst, a, n, bsz::mask_for_bits(bitlength)); });
+}
+int bsz_op_and(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b, uint64_t n) {
+  return guard([&] { bsz::launch_bitwise(*ctx->dev, bsz::kAnd, dst, a, b, n); });
+}
+int bsz_op_or(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b, uint64_t n) {
+  return guard([&] { bsz::launch_bitwise(*ctx->dev, bsz::kOr, dst, a, b, n); });
+}
+int bsz_op_xor(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b, uint64_t n) {
+  return guard([&] { bsz::launch_bitwise(*ctx->dev, bsz::kXor, dst, a, b, n); });
+}
+int bsz_op_andnot(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b, uint64_t n) {
+  return guard([&] { bsz::launch_bitwise(*ctx->dev, bsz::kAndNot, dst, a, b, n); });
+}
+int bsz_op_add(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b, uint64_t n,
+               int64_t bitlength) {
+  return guard([&] { bsz::launch_add(*ctx->dev, dst, a, b, n, bsz::mask_for_bits(bitlength)); });
+}
+int bsz_op_shl(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, uint64_t k, uint64_t n,
+               int64_t bitlength) {
+  return guard([&] {
+    bsz::launch_shl(*ctx->dev, dst, a, static_cast<int64_t>(std::min<uint64_t>(k, uint64_t(1) << 62)), n,
+                    bsz::mask_for_bits(bitlength));
+  });
+}
+int bsz_op_shr(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, uint64_t k, uint64_t n, int tail) {
+  return guard([&] {
+    bsz::launch_shr(*ctx->dev, dst, a, static_cast<int64_t>(std::min<uint64_t>(k, uint64_t(1) << 62)), n,
+                    tail ? ~uint64_t(0) : 0);
+  });
+}
+int bsz_op_popcount(bsz_ctx* ctx, const uint64_t* a, uint64_t n, uint64_t* result) {
+  return guard([&] {
+    bsz::Device& dev = *ctx->dev;
+    auto* slot = static_cast<unsigned long long*>(dev.scratch(256));
+    BSZ_CUDA(cudaMemsetAsync(slot, 0, 8, dev.stream()));
+    bsz::launch_popcount(dev, a, n, slot);
+    BSZ_CUDA(cudaMemcpyAsync(result, slot, 8, cudaMemcpyDeviceToHost, dev.stream()));
+    dev.sync();
+  });
+}
+int bsz_op_is_nonzero(bsz_ctx* ctx, const uint64_t* a, uint64_t n, int* result) {
+  return guard([&] {
+    bsz::Device& dev = *ctx->dev;
+    auto* flag = static_cast<unsigned int*>(dev.scratch(256));
+    BSZ_CUDA(cudaMemsetAsync(flag, 0, 4, dev.stream()));
+    bsz::launch_any(dev, a, n, flag);
+    unsigned int h = 0;
+    BSZ_CUDA(cudaMemcpyAsync(&h, flag, 4, cudaMemcpyDeviceToHost, dev.stream()));
+    dev.sync();
+    *result = h != 0;
+  });
+}
+
+}  // extern "C"

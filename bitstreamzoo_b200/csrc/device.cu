@@ -1,0 +1,133 @@
+// Device context: stream, buffer cache, scratch, error word.
+#include "device.h"
+
+#include <algorithm>
+
+namespace bsz {
+
+DevStream::~DevStream() {
+  if (dev && p) dev->release(this);
+}
+
+Device::Device(int ordinal) : ordinal_(ordinal) {
+  BSZ_CUDA(cudaSetDevice(ordinal));
+  cudaDeviceProp prop;
+  BSZ_CUDA(cudaGetDeviceProperties(&prop, ordinal));
+  if (prop.major < 10)
+    throw CudaError("bitstreamzoo_b200 needs an sm_100 (Blackwell B200) device; device " +
+                    std::to_string(ordinal) + " is " + prop.name);
+  sm_count_ = prop.multiProcessorCount;
+  BSZ_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  BSZ_CUDA(cudaMalloc(&d_err_, 256));
+  ++n_mallocs;
+  BSZ_CUDA(cudaMemsetAsync(d_err_, 0, 256, stream_));
+}
+
+Device::~Device() {
+  cudaSetDevice(ordinal_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto& kv : all_) cudaFree(kv.first);
+  if (d_scan_) cudaFree(d_scan_);
+  if (d_err_) cudaFree(d_err_);
+  if (d_scratch_) cudaFree(d_scratch_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void* Device::raw_alloc(size_t bytes) {
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    trim_cache();
+    e = cudaMalloc(&p, bytes);
+  }
+  if (e != cudaSuccess)
+    throw CudaError(std::string("cudaMalloc(") + std::to_string(bytes) +
+                    ") failed: " + cudaGetErrorString(e) +
+                    (e == cudaErrorMemoryAllocation ? " (out of memory)" : ""));
+  ++n_mallocs;
+  all_.push_back({p, bytes});
+  return p;
+}
+
+BufRef Device::alloc_stream(int64_t n_words) {
+  // Round to 256 bytes so vector loops may run over whole 16-byte pairs.
+  size_t bytes = (static_cast<size_t>(std::max<int64_t>(n_words, 1)) * 8 + 255) & ~size_t(255);
+  void* p = nullptr;
+  auto it = free_.find(bytes);
+  if (it != free_.end()) {
+    p = it->second;
+    free_.erase(it);
+  } else {
+    p = raw_alloc(bytes);
+  }
+  auto s = std::make_shared<DevStream>();
+  s->p = static_cast<uint64_t*>(p);
+  s->n_words = n_words;
+  s->bytes = bytes;
+  s->dev = this;
+  bytes_live += static_cast<int64_t>(bytes);
+  bytes_peak = std::max(bytes_peak, bytes_live);
+  return s;
+}
+
+void Device::release(DevStream* s) {
+  free_.emplace(s->bytes, s->p);
+  bytes_live -= static_cast<int64_t>(s->bytes);
+  s->p = nullptr;
+}
+
+void Device::trim_cache() {
+  cudaStreamSynchronize(stream_);
+  for (auto& kv : free_) {
+    cudaFree(kv.second);
+    all_.erase(std::remove_if(all_.begin(), all_.end(),
+                              [&](const std::pair<void*, size_t>& a) { return a.first == kv.second; }),
+               all_.end());
+  }
+  free_.clear();
+}
+
+uint32_t* Device::scan_state(int64_t n_u32) {
+  if (n_u32 > scan_cap_) {
+    if (d_scan_) {
+      BSZ_CUDA(cudaStreamSynchronize(stream_));
+      BSZ_CUDA(cudaFree(d_scan_));
+    }
+    int64_t cap = std::max<int64_t>(n_u32, 4096);
+    BSZ_CUDA(cudaMalloc(&d_scan_, static_cast<size_t>(cap) * 4));
+    ++n_mallocs;
+    scan_cap_ = cap;
+  }
+  BSZ_CUDA(cudaMemsetAsync(d_scan_, 0, static_cast<size_t>(n_u32) * 4, stream_));
+  return d_scan_;
+}
+
+void* Device::scratch(size_t bytes) {
+  if (bytes > scratch_cap_) {
+    if (d_scratch_) {
+      BSZ_CUDA(cudaStreamSynchronize(stream_));
+      BSZ_CUDA(cudaFree(d_scratch_));
+    }
+    size_t cap = std::max<size_t>(bytes, 1 << 16);
+    BSZ_CUDA(cudaMalloc(&d_scratch_, cap));
+    ++n_mallocs;
+    scratch_cap_ = cap;
+  }
+  return d_scratch_;
+}
+
+uint32_t Device::take_error() {
+  uint32_t h = 0;
+  BSZ_CUDA(cudaMemcpyAsync(&h, d_err_, 4, cudaMemcpyDeviceToHost, stream_));
+  BSZ_CUDA(cudaStreamSynchronize(stream_));
+  if (h) BSZ_CUDA(cudaMemsetAsync(d_err_, 0, 4, stream_));
+  return h;
+}
+
+void Device::sync() {
+  BSZ_CUDA(cudaStreamSynchronize(stream_));
+  BSZ_CUDA(cudaGetLastError());
+}
+
+}  // namespace bsz

@@ -1,0 +1,129 @@
+// Device runtime: one CUDA stream per context, a size-keyed cache of stream
+// buffers (no cudaMalloc/cudaFree on the steady-state path), popcount slots,
+// look-back scratch for the carry scan, and a device error word that bounded
+// spin-waits write instead of hanging.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace bsz {
+
+struct CudaError : std::runtime_error { using std::runtime_error::runtime_error; };
+
+#define BSZ_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      throw ::bsz::CudaError(std::string(#call) + " failed: " + cudaGetErrorString(e_) + \
+                             (e_ == cudaErrorMemoryAllocation ? " (out of memory)" : "")); \
+  } while (0)
+
+// Device error word bits (set by kernels, read by the host after a sync).
+enum : uint32_t {
+  kErrLookbackTimeout = 1u << 0,   // a carry look-back spin hit its limit
+  kErrFusedTimeout = 1u << 1,      // a fused-kernel boundary wait hit its limit
+  kErrFusedOverflow = 1u << 2,     // fused kernel: halo/state capacity exceeded
+};
+
+class Device;
+
+// A device stream buffer of n_words uint64 words (256-byte aligned).  Freed
+// back into the owning Device's cache; the memory is reused in stream order.
+struct DevStream {
+  uint64_t* p = nullptr;
+  int64_t n_words = 0;
+  size_t bytes = 0;
+  Device* dev = nullptr;
+  DevStream() = default;
+  DevStream(const DevStream&) = delete;
+  DevStream& operator=(const DevStream&) = delete;
+  ~DevStream();
+};
+using BufRef = std::shared_ptr<DevStream>;
+
+class Device {
+ public:
+  explicit Device(int ordinal);
+  ~Device();
+  Device(const Device&) = delete;
+  Device& operator=(const Device&) = delete;
+
+  int ordinal() const { return ordinal_; }
+  cudaStream_t stream() const { return stream_; }
+  int sm_count() const { return sm_count_; }
+
+  BufRef alloc_stream(int64_t n_words);
+  void release(DevStream* s);
+  void trim_cache();
+
+  // Look-back scratch: >= n_words_needed uint32 words, zeroed on the stream.
+  uint32_t* scan_state(int64_t n_u32);
+  uint32_t* error_word() const { return d_err_; }
+  // Copies the error word to the host (synchronizes the stream) and clears it.
+  uint32_t take_error();
+  void sync();
+
+  // Counters reported in the bsim_cuda JSON.
+  int64_t n_launches = 0;
+  int64_t n_mallocs = 0;
+  int64_t bytes_live = 0;
+  int64_t bytes_peak = 0;
+
+  // Untyped device scratch (cached; grows).
+  void* scratch(size_t bytes);
+
+ private:
+  int ordinal_;
+  int sm_count_ = 148;
+  cudaStream_t stream_ = nullptr;
+  std::multimap<size_t, void*> free_;   // bytes -> cached block
+  std::vector<std::pair<void*, size_t>> all_;
+  uint32_t* d_scan_ = nullptr;
+  int64_t scan_cap_ = 0;
+  uint32_t* d_err_ = nullptr;
+  void* d_scratch_ = nullptr;
+  size_t scratch_cap_ = 0;
+  void* raw_alloc(size_t bytes);
+};
+
+// ---------------------------------------------------------------------------
+// Plain per-op kernels (kernels.cu).  All launch asynchronously on
+// dev.stream().  ``last_mask`` clears the bits at and above the bitlength in
+// the last word, as the normative semantics mask ~, + and <<.
+// Pointer arguments must be 16-byte aligned for the vector path; unaligned
+// pointers take a scalar path.
+enum BitOp : int { kAnd = 0, kOr = 1, kXor = 2, kAndNot = 3 };
+
+void launch_bitwise(Device& dev, int op, uint64_t* d, const uint64_t* a, const uint64_t* b,
+                    int64_t n);
+void launch_not(Device& dev, uint64_t* d, const uint64_t* a, int64_t n, uint64_t last_mask);
+void launch_shl(Device& dev, uint64_t* d, const uint64_t* a, int64_t k, int64_t n,
+                uint64_t last_mask);
+void launch_shr(Device& dev, uint64_t* d, const uint64_t* a, int64_t k, int64_t n,
+                uint64_t fill);
+void launch_add(Device& dev, uint64_t* d, const uint64_t* a, const uint64_t* b, int64_t n,
+                uint64_t last_mask);
+// Same carry scan with caller-provided look-back state: ``state`` must hold
+// add_state_words(n) zeroed uint32 words.
+void launch_add_with_state(Device& dev, uint64_t* d, const uint64_t* a, const uint64_t* b,
+                           int64_t n, uint64_t last_mask, uint32_t* state);
+int64_t add_state_words(int64_t n);
+void launch_popcount(Device& dev, const uint64_t* a, int64_t n,
+                     unsigned long long* slot);
+void launch_any(Device& dev, const uint64_t* a, int64_t n, unsigned int* flag);
+void launch_fill(Device& dev, uint64_t* d, int64_t n, uint64_t value, uint64_t last_value);
+void launch_copy(Device& dev, uint64_t* d, const uint64_t* a, int64_t n);
+
+inline uint64_t mask_for_bits(int64_t nbits) {
+  int r = static_cast<int>(nbits & 63);
+  return r ? ((uint64_t(1) << r) - 1) : ~uint64_t(0);
+}
+
+}  // namespace bsz

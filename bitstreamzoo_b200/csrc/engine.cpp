@@ -1,0 +1,742 @@
+// Executor implementation (see engine.h).
+#include "engine.h"
+
+#include <algorithm>
+#include <chrono>
+#include <functional>
+
+#include "fused.h"
+
+namespace bsz {
+namespace {
+
+constexpr int kMaxWhileIters = 10000;          // simulator/pythonsim/interpreter.py:20
+constexpr int64_t kSlotChunk = 1 << 16;
+
+using Bits = std::vector<uint64_t>;
+inline bool bit(const Bits& b, int i) { return (b[i >> 6] >> (i & 63)) & 1u; }
+inline void set_bit(Bits& b, int i) { b[i >> 6] |= uint64_t(1) << (i & 63); }
+inline void clr_bit(Bits& b, int i) { b[i >> 6] &= ~(uint64_t(1) << (i & 63)); }
+inline void or_into(Bits& d, const Bits& s) {
+  for (size_t i = 0; i < d.size(); ++i) d[i] |= s[i];
+}
+
+bool commutative(NOp op) {
+  return op == NOp::And || op == NOp::Or || op == NOp::Xor || op == NOp::Add;
+}
+
+}  // namespace
+
+Executor::Executor(Device& dev, const Program& prog, int64_t bitlength, ExecOptions opt)
+    : dev_(dev), prog_(prog), opt_(opt) {
+  N_ = bitlength;
+  nw_ = std::max<int64_t>(1, (bitlength + 63) / 64);
+  if (bitlength <= 0) N_ = 64 * nw_;   // no bitlength: bounded by the storage width
+  last_mask_ = mask_for_bits(N_);
+  const size_t nn = prog.names.size();
+  var_.assign(nn, -1);
+  ints_.assign(nn, IntV{});
+  int_def_.assign(nn, 0);
+  arrs_.resize(nn);
+  zero_ = mk_raw(NOp::Zero, -1, -1, 0, 0);
+  ones_mask_ = mk_raw(NOp::OnesMask, -1, -1, 0, 0);
+  all_ones_ = mk_raw(NOp::AllOnes, -1, -1, 0, 1);
+  // Inputs that are not bound read as ZERO (interpreter.py:232-238).
+  for (int id : prog.inputs) var_[id] = zero_;
+  if (opt_.mode == ExecMode::Fused) {
+    opt_.simplify = true;
+    fused_ = std::make_unique<FusedBackend>(dev_, opt_);
+  }
+  BSZ_CUDA(cudaMalloc(&d_flag_, 256));
+  ++dev_.n_mallocs;
+  compute_liveness();
+}
+
+Executor::~Executor() {
+  cudaStreamSynchronize(dev_.stream());
+  if (d_flag_) cudaFree(d_flag_);
+  if (d_slots_) cudaFree(d_slots_);
+}
+
+void Executor::set_param(int name, int64_t v) {
+  if (name < 0) return;
+  ints_[name] = IntV{v, -1};
+  int_def_[name] = 1;
+}
+
+void Executor::bind_input(int name, BufRef buf, uint8_t tail, bool clean) {
+  var_[name] = buf_node(std::move(buf), tail, clean);
+}
+
+void Executor::bind_input_array(int name, int64_t idx, BufRef buf, uint8_t tail, bool clean) {
+  if (!arrs_[name]) arrs_[name] = std::make_unique<Arr>();
+  Arr& a = *arrs_[name];
+  a.defined = true;
+  a.elems[idx] = buf_node(std::move(buf), tail, clean);
+  if (var_[name] == zero_) var_[name] = -1;   // it is an array, not a scalar input
+}
+
+void Executor::bind_broadcast(int name, const std::vector<uint8_t>& ones) {
+  if (!arrs_[name]) arrs_[name] = std::make_unique<Arr>();
+  Arr& a = *arrs_[name];
+  a.defined = true;
+  a.broadcast = true;
+  a.bcast = ones;
+  if (var_[name] == zero_) var_[name] = -1;
+}
+
+// ------------------------------------------------------------------ graph --
+
+int Executor::mk_raw(NOp op, int a, int b, int64_t k, uint8_t tail) {
+  Node n;
+  n.op = op;
+  n.a = a;
+  n.b = b;
+  n.k = k;
+  n.tail = tail;
+  auto cl = [&](int x) { return x >= 0 && nodes_[x].clean; };
+  switch (op) {
+    case NOp::Zero: case NOp::OnesMask: case NOp::Not: case NOp::Add: case NOp::Shl:
+    case NOp::AndNot:
+      n.clean = 1; break;
+    case NOp::And: n.clean = cl(a) || cl(b); break;
+    case NOp::Or: case NOp::Xor: n.clean = cl(a) && cl(b); break;
+    case NOp::Shr: n.clean = cl(a); break;
+    default: n.clean = 0; break;
+  }
+  nodes_.push_back(std::move(n));
+  return static_cast<int>(nodes_.size()) - 1;
+}
+
+int Executor::buf_node(BufRef buf, uint8_t tail, bool clean) {
+  int id = mk_raw(NOp::Buf, -1, -1, 0, tail);
+  nodes_[id].buf = std::move(buf);
+  nodes_[id].clean = clean && tail == 0;
+  return id;
+}
+
+bool Executor::pending(int node) const {
+  const Node& n = nodes_[node];
+  return n.op != NOp::Buf && n.op != NOp::Zero && n.op != NOp::OnesMask &&
+         n.op != NOp::AllOnes && !n.buf;
+}
+
+int Executor::mk(NOp op, int a, int b, int64_t k) {
+  const uint8_t ta = a >= 0 ? nodes_[a].tail : 0, tb = b >= 0 ? nodes_[b].tail : 0;
+  uint8_t tail = 0;
+  switch (op) {
+    case NOp::And: tail = ta & tb; break;
+    case NOp::Or: tail = ta | tb; break;
+    case NOp::Xor: tail = ta ^ tb; break;
+    case NOp::Shr: tail = ta; break;
+    default: tail = 0; break;
+  }
+  if (opt_.simplify) {
+    auto is = [&](int x, NOp o) { return x >= 0 && nodes_[x].op == o; };
+    auto clean = [&](int x) { return nodes_[x].clean != 0; };
+    if (commutative(op) && b >= 0 && a > b) std::swap(a, b);
+    switch (op) {
+      case NOp::And:
+        if (a == b) return a;
+        if (is(a, NOp::Zero) || is(b, NOp::Zero)) return zero_;
+        if (is(a, NOp::AllOnes)) return b;
+        if (is(b, NOp::AllOnes)) return a;
+        if (is(a, NOp::OnesMask) && clean(b)) return b;
+        if (is(b, NOp::OnesMask) && clean(a)) return a;
+        break;
+      case NOp::Or:
+        if (a == b) return a;
+        if (is(a, NOp::Zero)) return b;
+        if (is(b, NOp::Zero)) return a;
+        if (is(a, NOp::AllOnes) || is(b, NOp::AllOnes)) return all_ones_;
+        if (is(a, NOp::OnesMask) && clean(b)) return a;
+        if (is(b, NOp::OnesMask) && clean(a)) return b;
+        break;
+      case NOp::Xor:
+        if (a == b) return zero_;
+        if (is(a, NOp::Zero)) return b;
+        if (is(b, NOp::Zero)) return a;
+        break;
+      case NOp::Not:
+        if (is(a, NOp::Zero)) return ones_mask_;
+        if (is(a, NOp::OnesMask) || is(a, NOp::AllOnes)) return zero_;
+        if (is(a, NOp::Not) && clean(nodes_[a].a)) return nodes_[a].a;
+        break;
+      case NOp::Add:
+        if (is(a, NOp::Zero) && clean(b)) return b;
+        if (is(b, NOp::Zero) && clean(a)) return a;
+        break;
+      case NOp::Shl:
+        if (is(a, NOp::Zero) || k >= N_) return zero_;
+        if (k == 0 && clean(a)) return a;
+        break;
+      case NOp::Shr:
+        if (k == 0) return a;
+        if (is(a, NOp::Zero) || is(a, NOp::AllOnes)) return a;
+        break;
+      default: break;
+    }
+    uint64_t key = (static_cast<uint64_t>(op) << 56) ^ (static_cast<uint64_t>(a + 1) << 28) ^
+                   static_cast<uint64_t>(b + 1) ^ (static_cast<uint64_t>(k) * 0x9E3779B97F4A7C15ull);
+    auto it = cse_.find(key);
+    if (it != cse_.end()) {
+      const Node& m = nodes_[it->second];
+      if (m.op == op && m.a == a && m.b == b && m.k == k) return it->second;
+    }
+    int id = mk_raw(op, a, b, k, tail);
+    cse_[key] = id;
+    return id;
+  }
+  return mk_raw(op, a, b, k, tail);
+}
+
+// ------------------------------------------------------------------ walk ---
+
+void Executor::count(const char* op) {
+  ++op_count;
+  ++op_mix[op];
+}
+
+int Executor::read_var(int name) {
+  int n = var_[name];
+  if (n >= 0) return n;
+  if (n == -2)
+    throw RuntimeError("internal: variable '" + prog_.names[name] + "' read after being judged dead");
+  throw RuntimeError("undefined stream variable: " + prog_.names[name]);
+}
+
+int Executor::elem(const SExpr& e) {
+  int64_t idx = force(ival(*e.index));
+  Arr* a = arrs_[e.name].get();
+  if (!a || !a->defined) throw RuntimeError("undefined array: " + prog_.names[e.name]);
+  auto it = a->elems.find(idx);
+  if (it != a->elems.end()) return it->second;
+  if (a->broadcast && idx >= 0 && idx < static_cast<int64_t>(a->bcast.size()))
+    return a->bcast[idx] ? all_ones_ : zero_;
+  return zero_;
+}
+
+// Operand read (interpreter.py:70-84): ONES is the N-bit mask here.
+int Executor::operand(const SExpr& e) {
+  switch (e.kind) {
+    case SExpr::Var: return read_var(e.name);
+    case SExpr::Zero: return zero_;
+    case SExpr::Ones: return ones_mask_;
+    case SExpr::Elem: return elem(e);
+    default: throw RuntimeError("internal: operand is not a primary");
+  }
+}
+
+// Right-hand side (interpreter.py:150-218): a copy of ONES is all ones with
+// tail 1; ~ + << are masked (the mask is applied by the kernels).
+int Executor::rhs(const SExpr& e) {
+  switch (e.kind) {
+    case SExpr::Var: return read_var(e.name);
+    case SExpr::Zero: return zero_;
+    case SExpr::Ones: return all_ones_;
+    case SExpr::Elem: return elem(e);
+    case SExpr::Not: {
+      int a = operand(*e.a);
+      count("~");
+      return mk(NOp::Not, a);
+    }
+    case SExpr::Bin: {
+      int a = operand(*e.a);
+      int b = operand(*e.b);
+      NOp op = e.op == '&' ? NOp::And : e.op == '|' ? NOp::Or : e.op == '^' ? NOp::Xor : NOp::Add;
+      const char* name = e.op == '&' ? "&" : e.op == '|' ? "|" : e.op == '^' ? "^" : "+";
+      count(name);
+      return mk(op, a, b);
+    }
+    case SExpr::Shift: {
+      int a = operand(*e.a);
+      int64_t k = force(ival(*e.index));
+      if (k < 0) throw RuntimeError("negative shift count");
+      count(e.op == '<' ? "<<" : ">>");
+      return mk(e.op == '<' ? NOp::Shl : NOp::Shr, a, -1, k);
+    }
+  }
+  throw RuntimeError("internal: unknown stream expression");
+}
+
+Executor::IntV Executor::ival(const IExpr& e) {
+  switch (e.kind) {
+    case IExpr::Lit: return IntV{e.value, -1};
+    case IExpr::Var:
+      if (!int_def_[e.name]) throw RuntimeError("undefined int variable: " + prog_.names[e.name]);
+      return ints_[e.name];
+    case IExpr::Bin: {
+      IntV a = ival(*e.a), b = ival(*e.b);
+      if (a.e < 0 && b.e < 0) {
+        int64_t v = e.op == '+' ? a.v + b.v : e.op == '-' ? a.v - b.v : a.v * b.v;
+        return IntV{v, -1};
+      }
+      auto leaf = [&](const IntV& x) {
+        if (x.e >= 0) return x.e;
+        iexpr_.push_back(IE{'k', -1, -1, x.v});
+        return static_cast<int32_t>(iexpr_.size() - 1);
+      };
+      int32_t la = leaf(a), lb = leaf(b);
+      iexpr_.push_back(IE{e.op, la, lb, 0});
+      return IntV{0, static_cast<int32_t>(iexpr_.size() - 1)};
+    }
+    case IExpr::Pop: {
+      if (e.arg->kind != SExpr::Var) throw RuntimeError("popcount arg must be a variable");
+      return popcount(read_var(e.arg->name));
+    }
+  }
+  throw RuntimeError("internal: unknown int expression");
+}
+
+Executor::IntV Executor::popcount(int node) {
+  const Node& n = nodes_[node];
+  if (n.tail) throw RuntimeError("popcount on negative value (infinite bits set)");
+  count("popcount");
+  if (n.op == NOp::Zero) return IntV{0, -1};
+  if (n.op == NOp::OnesMask) return IntV{N_, -1};
+  ensure_slots(1);
+  int64_t slot = n_slots_++;
+  pending_pops_.push_back({node, slot});
+  iexpr_.push_back(IE{'s', -1, -1, slot});
+  return IntV{0, static_cast<int32_t>(iexpr_.size() - 1)};
+}
+
+int64_t Executor::eval_ie(int32_t e) {
+  const IE& x = iexpr_[e];
+  switch (x.op) {
+    case 'k': return x.v;
+    case 's': return static_cast<int64_t>(slot_val_[x.v]);
+    case '+': return eval_ie(x.a) + eval_ie(x.b);
+    case '-': return eval_ie(x.a) - eval_ie(x.b);
+    default: return eval_ie(x.a) * eval_ie(x.b);
+  }
+}
+
+int64_t Executor::force(const IntV& x) {
+  if (x.e < 0) return x.v;
+  resolve_slots();
+  return eval_ie(x.e);
+}
+
+bool Executor::nonzero(int node, const Stmt* at) {
+  const Node& n = nodes_[node];
+  if (n.tail) return true;                // negative value: nonzero
+  if (n.op == NOp::Zero) return false;
+  if (n.op == NOp::OnesMask || n.op == NOp::AllOnes) return N_ > 0;
+  int x = node;
+  auto it = at ? live_at_.find(at->id) : live_at_.end();
+  flush(it == live_at_.end() ? nullptr : &it->second, &x);
+  BSZ_CUDA(cudaMemsetAsync(d_flag_, 0, 4, dev_.stream()));
+  launch_any(dev_, nodes_[x].buf->p, nw_, d_flag_);
+  unsigned int h = 0;
+  BSZ_CUDA(cudaMemcpyAsync(&h, d_flag_, 4, cudaMemcpyDeviceToHost, dev_.stream()));
+  dev_.sync();
+  ++n_syncs;
+  if (uint32_t err = dev_.take_error()) throw RuntimeError("device error word " + std::to_string(err));
+  return h != 0;
+}
+
+void Executor::exec_block(const std::vector<Stmt>& v) {
+  for (const auto& s : v) exec(s);
+}
+
+void Executor::exec(const Stmt& s) {
+  switch (s.kind) {
+    case Stmt::LocalDecl:
+      var_[s.name] = s.e ? rhs(*s.e) : zero_;
+      break;
+    case Stmt::Assign:
+      var_[s.name] = rhs(*s.e);
+      break;
+    case Stmt::ArrayDecl: {
+      int64_t n = force(ival(*s.ie));
+      if (!arrs_[s.name]) arrs_[s.name] = std::make_unique<Arr>();
+      Arr& a = *arrs_[s.name];
+      a.defined = true;
+      a.broadcast = false;
+      a.bcast.clear();
+      a.elems.clear();
+      a.decl_size = std::max<int64_t>(n, 0);
+      break;
+    }
+    case Stmt::ArrayAssign: {
+      int64_t idx = force(ival(*s.ie));
+      int v = rhs(*s.e);
+      if (!arrs_[s.name]) arrs_[s.name] = std::make_unique<Arr>();
+      Arr& a = *arrs_[s.name];
+      a.defined = true;
+      a.elems[idx] = v;
+      break;
+    }
+    case Stmt::IntDecl:
+    case Stmt::IntAssign:
+      ints_[s.name] = ival(*s.ie);
+      int_def_[s.name] = 1;
+      break;
+    case Stmt::If:
+      if (nonzero(read_var(s.e->name), &s)) exec_block(s.body);
+      break;
+    case Stmt::While: {
+      for (int it = 0; it < kMaxWhileIters; ++it) {
+        if (!nonzero(read_var(s.e->name), &s)) return;
+        exec_block(s.body);
+      }
+      throw RuntimeError("while loop exceeded 10000 iterations");
+    }
+    case Stmt::For: {
+      int64_t lo = force(ival(*s.ie));
+      int64_t hi = force(ival(*s.ie2));
+      for (int64_t i = lo; i < hi; ++i) {
+        ints_[s.name] = IntV{i, -1};
+        int_def_[s.name] = 1;
+        exec_block(s.body);
+      }
+      break;
+    }
+  }
+}
+
+void Executor::run() {
+  exec_block(prog_.stmts);
+  flush(&live_end_, nullptr);
+  resolve_slots();
+  // Outputs bound to constants get a buffer so the caller can read them.
+  auto materialize = [&](int& node) {
+    Node& n = nodes_[node];
+    if (n.op == NOp::Buf || n.buf) return;
+    BufRef b = dev_.alloc_stream(nw_);
+    if (n.op == NOp::Zero) launch_fill(dev_, b->p, nw_, 0, 0);
+    else if (n.op == NOp::OnesMask) launch_fill(dev_, b->p, nw_, ~uint64_t(0), last_mask_);
+    else launch_fill(dev_, b->p, nw_, ~uint64_t(0), ~uint64_t(0));
+    node = buf_node(b, n.tail, n.clean);
+  };
+  for (int id : prog_.outputs) {
+    if (var_[id] >= 0) materialize(var_[id]);
+    if (arrs_[id])
+      for (auto& kv : arrs_[id]->elems) materialize(kv.second);
+  }
+  if (uint32_t err = dev_.take_error()) throw RuntimeError("device error word " + std::to_string(err));
+}
+
+// ----------------------------------------------------------------- flush ---
+
+void Executor::flush(const Bits* live, int* extra) {
+  const int n_nodes = static_cast<int>(nodes_.size());
+  std::vector<uint8_t> is_target(n_nodes, 0), need(n_nodes, 0);
+  Segment seg;
+  auto add_target = [&](int n) {
+    if (n >= 0 && pending(n) && !is_target[n]) {
+      is_target[n] = 1;
+      seg.outputs.push_back(n);
+    }
+  };
+  for (size_t v = 0; v < var_.size(); ++v) {
+    int n = var_[v];
+    if (n < 0 || !pending(n)) continue;
+    if (!live || bit(*live, static_cast<int>(v))) add_target(n);
+    else var_[v] = -2;
+  }
+  for (auto& a : arrs_)
+    if (a) for (auto& kv : a->elems) add_target(kv.second);
+  if (extra) add_target(*extra);
+  std::vector<int> stack(seg.outputs.begin(), seg.outputs.end());
+  for (auto& p : pending_pops_) stack.push_back(p.first);
+  while (!stack.empty()) {
+    int n = stack.back();
+    stack.pop_back();
+    if (need[n]) continue;
+    need[n] = 1;
+    const Node& x = nodes_[n];
+    if (!pending(n)) continue;
+    if (x.a >= 0) stack.push_back(x.a);
+    if (x.b >= 0) stack.push_back(x.b);
+  }
+  for (int i = 0; i < n_nodes; ++i) {
+    if (!need[i]) continue;
+    if (pending(i)) seg.order.push_back(i);
+    else seg.inputs.push_back(i);
+  }
+  for (auto& p : pending_pops_) seg.pops.push_back({p.first, p.second - slot_base_});
+  if (!seg.order.empty() || !seg.pops.empty()) {
+    ++n_segments;
+    if (opt_.mode == ExecMode::Fused) {
+      for (int i : seg.inputs) const_ptr(i);
+      fused_->run(nodes_, seg, N_, nw_, d_slots_, &compile_ms);
+    } else {
+      run_plain(seg);
+    }
+  }
+  pending_pops_.clear();
+  max_live_buffers = std::max(max_live_buffers, live_buffer_count());
+  compact(extra);
+}
+
+int64_t Executor::live_buffer_count() const {
+  int64_t c = 0;
+  for (const auto& n : nodes_)
+    if (n.buf) ++c;
+  return c;
+}
+
+const uint64_t* Executor::const_ptr(int node) {
+  Node& n = nodes_[node];
+  if (n.buf) return n.buf->p;
+  BufRef* slot = nullptr;
+  uint64_t v = 0, last = 0;
+  switch (n.op) {
+    case NOp::Zero: slot = &c_zero_; v = 0; last = 0; break;
+    case NOp::OnesMask: slot = &c_mask_; v = ~uint64_t(0); last = last_mask_; break;
+    case NOp::AllOnes: slot = &c_all_; v = ~uint64_t(0); last = ~uint64_t(0); break;
+    default: throw RuntimeError("internal: operand not materialized");
+  }
+  if (!*slot) {
+    *slot = dev_.alloc_stream(nw_);
+    launch_fill(dev_, (*slot)->p, nw_, v, last);
+  }
+  return (*slot)->p;
+}
+
+void Executor::run_plain(const Segment& seg) {
+  const int n_nodes = static_cast<int>(nodes_.size());
+  std::vector<int> uses(n_nodes, 0);
+  std::vector<uint8_t> keep(n_nodes, 0);
+  for (int o : seg.outputs) keep[o] = 1;
+  std::vector<std::vector<int64_t>> pops_of(n_nodes);
+  for (auto& p : seg.pops) pops_of[p.first].push_back(p.second);
+  for (int id : seg.order) {
+    const Node& n = nodes_[id];
+    if (n.a >= 0 && pending(n.a)) ++uses[n.a];
+    if (n.b >= 0 && pending(n.b)) ++uses[n.b];
+  }
+  auto launch_pops = [&](int id) {
+    for (int64_t slot : pops_of[id])
+      launch_popcount(dev_, nodes_[id].buf ? nodes_[id].buf->p : const_ptr(id), nw_, d_slots_ + slot);
+  };
+  for (int i : seg.inputs) launch_pops(i);
+  for (int id : seg.order) {
+    Node& n = nodes_[id];
+    const uint64_t* A = n.a >= 0 ? (nodes_[n.a].buf ? nodes_[n.a].buf->p : const_ptr(n.a)) : nullptr;
+    const uint64_t* B = n.b >= 0 ? (nodes_[n.b].buf ? nodes_[n.b].buf->p : const_ptr(n.b)) : nullptr;
+    BufRef out = dev_.alloc_stream(nw_);
+    uint64_t* D = out->p;
+    switch (n.op) {
+      case NOp::Not: launch_not(dev_, D, A, nw_, last_mask_); break;
+      case NOp::And: launch_bitwise(dev_, kAnd, D, A, B, nw_); break;
+      case NOp::Or: launch_bitwise(dev_, kOr, D, A, B, nw_); break;
+      case NOp::Xor: launch_bitwise(dev_, kXor, D, A, B, nw_); break;
+      case NOp::AndNot: launch_bitwise(dev_, kAndNot, D, A, B, nw_); break;
+      case NOp::Add: launch_add(dev_, D, A, B, nw_, last_mask_); break;
+      case NOp::Shl: launch_shl(dev_, D, A, n.k, nw_, last_mask_); break;
+      case NOp::Shr:
+        launch_shr(dev_, D, A, n.k, nw_, nodes_[n.a].tail ? ~uint64_t(0) : 0);
+        break;
+      default: throw RuntimeError("internal: unexpected node in plain segment");
+    }
+    n.buf = std::move(out);
+    launch_pops(id);
+    for (int operand : {n.a, n.b}) {
+      if (operand >= 0 && pending(operand) == false && nodes_[operand].op != NOp::Buf &&
+          uses[operand] > 0 && --uses[operand] == 0 && !keep[operand])
+        nodes_[operand].buf.reset();
+    }
+  }
+  max_live_buffers = std::max(max_live_buffers, live_buffer_count());
+}
+
+void Executor::compact(int* extra) {
+  std::vector<Node> old;
+  old.swap(nodes_);
+  cse_.clear();
+  std::vector<int> remap(old.size(), -1);
+  zero_ = mk_raw(NOp::Zero, -1, -1, 0, 0);
+  ones_mask_ = mk_raw(NOp::OnesMask, -1, -1, 0, 0);
+  all_ones_ = mk_raw(NOp::AllOnes, -1, -1, 0, 1);
+  auto map = [&](int n) -> int {
+    if (n < 0) return n;
+    if (remap[n] >= 0) return remap[n];
+    const Node& x = old[n];
+    int id;
+    switch (x.op) {
+      case NOp::Zero: id = zero_; break;
+      case NOp::OnesMask: id = ones_mask_; break;
+      case NOp::AllOnes: id = all_ones_; break;
+      default:
+        if (!x.buf) throw RuntimeError("internal: live value was not materialized");
+        id = buf_node(x.buf, x.tail, x.clean);
+    }
+    remap[n] = id;
+    return id;
+  };
+  for (auto& v : var_) v = map(v);
+  for (auto& a : arrs_)
+    if (a) for (auto& kv : a->elems) kv.second = map(kv.second);
+  if (extra) *extra = map(*extra);
+}
+
+// ----------------------------------------------------------------- slots ---
+
+void Executor::ensure_slots(int64_t need) {
+  if (slot_cap_ == 0) {
+    slot_cap_ = kSlotChunk;
+    BSZ_CUDA(cudaMalloc(&d_slots_, static_cast<size_t>(slot_cap_) * 8));
+    ++dev_.n_mallocs;
+    BSZ_CUDA(cudaMemsetAsync(d_slots_, 0, static_cast<size_t>(slot_cap_) * 8, dev_.stream()));
+  }
+  if (n_slots_ - slot_base_ + need > slot_cap_) {
+    resolve_slots();
+    BSZ_CUDA(cudaMemsetAsync(d_slots_, 0, static_cast<size_t>(slot_cap_) * 8, dev_.stream()));
+    slot_base_ = n_slots_;
+  }
+  if (static_cast<int64_t>(slot_val_.size()) < n_slots_ + need) slot_val_.resize(n_slots_ + need + 1024);
+}
+
+void Executor::resolve_slots() {
+  if (!pending_pops_.empty()) flush(nullptr, nullptr);
+  if (resolved_upto_ < n_slots_) {
+    int64_t from = resolved_upto_ - slot_base_;
+    int64_t cnt = n_slots_ - resolved_upto_;
+    BSZ_CUDA(cudaMemcpyAsync(slot_val_.data() + resolved_upto_, d_slots_ + from,
+                             static_cast<size_t>(cnt) * 8, cudaMemcpyDeviceToHost, dev_.stream()));
+    dev_.sync();
+    ++n_syncs;
+    resolved_upto_ = n_slots_;
+  }
+}
+
+// -------------------------------------------------------------- liveness ---
+// Backward dataflow over the AST: for every if/while statement, the scalar
+// stream names that may be read at or after it (loops iterate to a fixed
+// point).  At a flush only those values are materialized; temporaries that
+// are dead there are never computed.
+
+void Executor::compute_liveness() {
+  const int nn = static_cast<int>(prog_.names.size());
+  const size_t nb = (static_cast<size_t>(nn) + 63) / 64;
+  auto scalar = [&](int id) { return id >= 0 && !prog_.is_array[id]; };
+  std::function<void(const IExpr&, Bits&)> gen_i;
+  std::function<void(const SExpr&, Bits&)> gen_s = [&](const SExpr& e, Bits& L) {
+    switch (e.kind) {
+      case SExpr::Var: if (scalar(e.name)) set_bit(L, e.name); break;
+      case SExpr::Elem: gen_i(*e.index, L); break;
+      case SExpr::Not: gen_s(*e.a, L); break;
+      case SExpr::Bin: gen_s(*e.a, L); gen_s(*e.b, L); break;
+      case SExpr::Shift: gen_s(*e.a, L); gen_i(*e.index, L); break;
+      default: break;
+    }
+  };
+  gen_i = [&](const IExpr& e, Bits& L) {
+    if (e.kind == IExpr::Pop) gen_s(*e.arg, L);
+    else if (e.kind == IExpr::Bin) { gen_i(*e.a, L); gen_i(*e.b, L); }
+  };
+  std::function<Bits(const std::vector<Stmt>&, Bits)> block = [&](const std::vector<Stmt>& v, Bits L) {
+    for (auto it = v.rbegin(); it != v.rend(); ++it) {
+      const Stmt& s = *it;
+      switch (s.kind) {
+        case Stmt::LocalDecl:
+        case Stmt::Assign:
+          if (scalar(s.name)) clr_bit(L, s.name);
+          if (s.e) gen_s(*s.e, L);
+          break;
+        case Stmt::ArrayAssign: gen_s(*s.e, L); gen_i(*s.ie, L); break;
+        case Stmt::ArrayDecl: gen_i(*s.ie, L); break;
+        case Stmt::IntDecl:
+        case Stmt::IntAssign: gen_i(*s.ie, L); break;
+        case Stmt::If: {
+          Bits in = block(s.body, L);
+          or_into(L, in);
+          set_bit(L, s.e->name);
+          live_at_[s.id] = L;
+          break;
+        }
+        case Stmt::While: {
+          const Bits out = L;
+          Bits X = out;
+          set_bit(X, s.e->name);
+          for (int guard = 0; guard < 1000; ++guard) {
+            Bits B = block(s.body, X);
+            Bits Xn = out;
+            or_into(Xn, B);
+            set_bit(Xn, s.e->name);
+            if (Xn == X) break;
+            X = std::move(Xn);
+          }
+          live_at_[s.id] = X;
+          L = X;
+          break;
+        }
+        case Stmt::For: {
+          gen_i(*s.ie, L);
+          gen_i(*s.ie2, L);
+          const Bits out = L;
+          Bits X = out;
+          for (int guard = 0; guard < 1000; ++guard) {
+            Bits B = block(s.body, X);
+            Bits Xn = out;
+            or_into(Xn, B);
+            if (Xn == X) break;
+            X = std::move(Xn);
+          }
+          L = X;
+          break;
+        }
+      }
+    }
+    return L;
+  };
+  live_end_.assign(nb, 0);
+  for (int id : prog_.outputs)
+    if (scalar(id)) set_bit(live_end_, id);
+  block(prog_.stmts, live_end_);
+}
+
+// --------------------------------------------------------------- results ---
+
+bool Executor::has_stream(int name) const { return name >= 0 && var_[name] >= 0; }
+
+BufRef Executor::stream_value(int name) {
+  if (!has_stream(name)) return nullptr;
+  Node& n = nodes_[var_[name]];
+  return n.buf;
+}
+
+uint8_t Executor::stream_tail(int name) const { return has_stream(name) ? nodes_[var_[name]].tail : 0; }
+
+bool Executor::has_array(int name) const {
+  return name >= 0 && arrs_[name] && arrs_[name]->defined;
+}
+
+std::vector<int64_t> Executor::array_indices(int name) const {
+  std::vector<int64_t> idx;
+  if (!has_array(name)) return idx;
+  const Arr& a = *arrs_[name];
+  for (int64_t i = 0; i < a.decl_size; ++i) idx.push_back(i);
+  if (a.broadcast)
+    for (int64_t i = 0; i < static_cast<int64_t>(a.bcast.size()); ++i) idx.push_back(i);
+  for (auto& kv : a.elems) idx.push_back(kv.first);
+  std::sort(idx.begin(), idx.end());
+  idx.erase(std::unique(idx.begin(), idx.end()), idx.end());
+  return idx;
+}
+
+BufRef Executor::array_value(int name, int64_t idx) {
+  if (!has_array(name)) return nullptr;
+  Arr& a = *arrs_[name];
+  auto it = a.elems.find(idx);
+  int node;
+  if (it != a.elems.end()) node = it->second;
+  else if (a.broadcast && idx >= 0 && idx < static_cast<int64_t>(a.bcast.size()))
+    node = a.bcast[idx] ? all_ones_ : zero_;
+  else node = zero_;
+  if (!nodes_[node].buf) const_ptr(node);
+  Node& n = nodes_[node];
+  if (n.buf) return n.buf;
+  return n.op == NOp::Zero ? c_zero_ : n.op == NOp::OnesMask ? c_mask_ : c_all_;
+}
+
+bool Executor::int_value(int name, int64_t* v) {
+  if (name < 0 || !int_def_[name]) return false;
+  *v = force(ints_[name]);
+  return true;
+}
+
+}  // namespace bsz

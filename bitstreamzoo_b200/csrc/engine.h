@@ -1,0 +1,172 @@
+// Executor: walks the program on the host and lowers stream statements into
+// an op DAG that runs on the GPU in segments.
+//
+// Replaces the reference's statement-at-a-time Interpreter<CudaBackend>
+// (simulator/csim/src/interpreter.inl:93-364), which launches one or more
+// kernels per DSL op and synchronizes for every popcount and condition.
+// Here stream values are DAG nodes; nothing runs until a value is needed on
+// the host (an if/while condition, a popcount that feeds a loop bound, shift
+// amount or array index, or the end of the program).  At that point the
+// pending DAG (after dead-code elimination against the live variables) is
+// executed as one segment, either
+//   * plain: one kernel per DSL operation, or
+//   * fused: one generated persistent kernel for the whole segment.
+// Popcounts are accumulated into device slots and read back once.
+//
+// Semantics are the normative Python ones (simulator/pythonsim/interpreter.py):
+// a stream is n = ceil(N/64) stored words plus a "tail" bit that every bit past
+// the stored words equals (Python's negative integers).  ~, + and << clear the
+// bits at and above N; & | ^ >> do not; ONES is the N-bit mask as an operand
+// but all-ones with tail 1 when copied; popcount of a value whose tail is 1 is
+// an error.  Tails never depend on data, so they are tracked on the host.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "device.h"
+#include "frontend.h"
+
+namespace bsz {
+
+struct RuntimeError : std::runtime_error { using std::runtime_error::runtime_error; };
+
+enum class NOp : uint8_t { Buf, Zero, OnesMask, AllOnes, Not, And, Or, Xor, AndNot, Add, Shl, Shr };
+
+struct Node {
+  NOp op = NOp::Zero;
+  int32_t a = -1, b = -1;
+  int64_t k = 0;          // shift amount
+  uint8_t tail = 0;       // bits past the stored words (0 or 1)
+  uint8_t clean = 0;      // known: stored bits at/above N are zero and tail is 0
+  BufRef buf;             // Buf nodes, and computed nodes once materialized
+};
+
+enum class ExecMode : int { Plain = 0, Fused = 1 };
+
+struct ExecOptions {
+  ExecMode mode = ExecMode::Plain;
+  bool simplify = false;        // algebraic folding + CSE (on in fused mode)
+  int fused_warps = 4;          // fused: warps per CTA
+  int fused_chunk_steps = 64;   // fused: 32-word steps per warp chunk
+  int fused_warmup_steps = 2;   // fused: speculative warm-up steps before a chunk
+  int fused_ctas_per_sm = 4;    // fused: grid = SMs * this (persistent)
+};
+
+// A segment handed to the plain or fused backend: nodes in topological order.
+struct Segment {
+  std::vector<int> order;                     // computed nodes, topological
+  std::vector<int> inputs;                    // Buf / constant nodes read
+  std::vector<int> outputs;                   // nodes to materialize
+  std::vector<std::pair<int, int64_t>> pops;  // (node, slot index)
+};
+
+class FusedBackend;
+
+class Executor {
+ public:
+  Executor(Device& dev, const Program& prog, int64_t bitlength, ExecOptions opt);
+  ~Executor();
+
+  int64_t bitlength() const { return N_; }
+  int64_t n_words() const { return nw_; }
+
+  void set_param(int name, int64_t v);
+  void bind_input(int name, BufRef buf, uint8_t tail, bool clean);
+  void bind_input_array(int name, int64_t idx, BufRef buf, uint8_t tail, bool clean);
+  void bind_broadcast(int name, const std::vector<uint8_t>& ones);   // element i: 1 = -1
+
+  void run();
+
+  // Results (valid after run()).
+  bool has_stream(int name) const;
+  BufRef stream_value(int name);                 // materialized buffer
+  uint8_t stream_tail(int name) const;
+  std::vector<int64_t> array_indices(int name) const;   // sorted; empty if absent
+  BufRef array_value(int name, int64_t idx);
+  bool has_array(int name) const;
+  bool int_value(int name, int64_t* v);
+
+  int64_t op_count = 0;
+  std::map<std::string, int64_t> op_mix;
+  int64_t n_segments = 0;
+  int64_t n_syncs = 0;
+  int64_t max_live_buffers = 0;
+  double compile_ms = 0.0;
+
+ private:
+  struct IntV { int64_t v = 0; int32_t e = -1; };
+  struct IE { char op; int32_t a, b; int64_t v; };
+  struct Arr {
+    bool defined = false;
+    bool broadcast = false;
+    std::vector<uint8_t> bcast;
+    int64_t decl_size = 0;          // indices [0, decl_size) exist (zero unless written)
+    std::map<int64_t, int> elems;   // index -> node
+  };
+
+  Device& dev_;
+  const Program& prog_;
+  int64_t N_, nw_;
+  uint64_t last_mask_;
+  ExecOptions opt_;
+
+  std::vector<Node> nodes_;
+  std::unordered_map<uint64_t, int> cse_;
+  int zero_ = -1, ones_mask_ = -1, all_ones_ = -1;
+  BufRef c_zero_, c_mask_, c_all_;
+
+  std::vector<int> var_;          // name -> node (-1 undefined, -2 dropped as dead)
+  std::vector<IntV> ints_;
+  std::vector<uint8_t> int_def_;
+  std::vector<std::unique_ptr<Arr>> arrs_;
+  std::vector<IE> iexpr_;
+
+  // popcount slots
+  unsigned long long* d_slots_ = nullptr;
+  int64_t slot_cap_ = 0, slot_base_ = 0, n_slots_ = 0;
+  std::vector<uint64_t> slot_val_;
+  std::vector<std::pair<int, int64_t>> pending_pops_;
+  int64_t resolved_upto_ = 0;
+
+  // liveness: stream names live at each if/while statement
+  std::unordered_map<int, std::vector<uint64_t>> live_at_;
+  std::vector<uint64_t> live_end_;
+
+  std::unique_ptr<FusedBackend> fused_;
+  unsigned int* d_flag_ = nullptr;
+
+  // walk
+  void exec_block(const std::vector<Stmt>& v);
+  void exec(const Stmt& s);
+  int rhs(const SExpr& e);
+  int operand(const SExpr& e);
+  int elem(const SExpr& e);
+  int read_var(int name);
+  IntV ival(const IExpr& e);
+  int64_t force(const IntV& x);
+  int64_t eval_ie(int32_t e);
+  bool nonzero(int node, const Stmt* at);
+  IntV popcount(int node);
+  void count(const char* op);
+
+  // graph
+  int mk(NOp op, int a = -1, int b = -1, int64_t k = 0);
+  int mk_raw(NOp op, int a, int b, int64_t k, uint8_t tail);
+  int buf_node(BufRef buf, uint8_t tail, bool clean);
+  bool pending(int node) const;
+  void flush(const std::vector<uint64_t>* live, int* extra);
+  void compact(int* extra);
+  void run_plain(const Segment& seg);
+  const uint64_t* const_ptr(int node);
+  void ensure_slots(int64_t need);
+  void resolve_slots();
+  void compute_liveness();
+  int64_t live_buffer_count() const;
+};
+
+}  // namespace bsz

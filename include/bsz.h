@@ -1,0 +1,142 @@
+/*
+ * bsz.h -- C ABI of the B200 bitstream executor (libbsz.so).
+ *
+ * Plain C types only (pointers, sizes, int64).  No exceptions cross this
+ * boundary: every function returns a status (0 = OK, nonzero = error; NULL
+ * for constructors) and bsz_last_error() returns the message of the last
+ * failure on the calling thread.  A context owns one CUDA stream and all
+ * device buffers it allocates; it is not thread-safe.
+ *
+ * Streams are little-endian arrays of uint64 words: bit i of a stream is bit
+ * (i % 64) of word (i / 64).  A stream of bitlength N has ceil(N/64) words.
+ * Beyond its stored words a stream carries a "tail" bit (0 or 1): the value
+ * of every higher bit, which is how the reference's normative Python
+ * semantics represent negative integers (infinitely many ones).
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *  - the bsim_cuda process contract  simulator/csim/src/main.cu:209-331
+ *    (argv + JSON on stdout)          -> bsz_run_case_json(), and the
+ *                                        bsim_cuda executable built on it
+ *  - Interpreter<Backend>::run        simulator/csim/src/interpreter.inl:234-364
+ *                                     -> bsz_compile / bsz_run_* / bsz_execute
+ *  - the CudaBackend data plane       simulator/csim/src/cuda_backend.cuh:16-229
+ *    (op_not/and/or/xor/add/shl/shr,   -> bsz_op_* entry points on device
+ *     op_popcount, op_is_nonzero)          pointers
+ */
+#ifndef BSZ_H_
+#define BSZ_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bsz_ctx bsz_ctx;
+typedef struct bsz_program bsz_program;
+typedef struct bsz_run bsz_run;
+
+/* Execution forms. */
+#define BSZ_MODE_PLAIN 0   /* one kernel per DSL operation */
+#define BSZ_MODE_FUSED 1   /* whole straight-line segments as one generated kernel */
+
+typedef struct bsz_stats {
+  int64_t op_count;          /* dynamic DSL op count (same counting as the reference) */
+  int64_t n_kernel_launches; /* kernels launched by this execution */
+  int64_t n_mallocs;         /* cudaMalloc calls made by the context so far */
+  int64_t n_segments;        /* device segments executed */
+  int64_t n_syncs;           /* host<->device synchronisations */
+  int64_t peak_bytes;        /* peak device bytes held in stream buffers */
+  int64_t max_live;          /* peak number of live stream buffers */
+  double kernel_ms;          /* CUDA-event time of the execution */
+  double compile_ms;         /* time spent generating/compiling fused kernels */
+} bsz_stats;
+
+/* ---- library ---------------------------------------------------------- */
+const char* bsz_version(void);
+const char* bsz_last_error(void);
+
+/* ---- context ---------------------------------------------------------- */
+/* Creates a context on CUDA device `device` (must be sm_100). */
+bsz_ctx* bsz_create(int device);
+void bsz_destroy(bsz_ctx* ctx);
+/* The context's cudaStream_t, as void*. */
+void* bsz_stream(bsz_ctx* ctx);
+int bsz_sync(bsz_ctx* ctx);
+
+/* ---- programs (replaces bs::parse, simulator/csim/src/parser.cpp:451-457) */
+/* Parses and validates DSL source.  NULL on ParseError / ThreeAddrError. */
+bsz_program* bsz_compile(bsz_ctx* ctx, const char* source, size_t len);
+void bsz_program_free(bsz_program* prog);
+/* Static op count for the given params (ast_liveness.cpp:629-727). */
+int64_t bsz_static_ops(bsz_program* prog, const char* const* param_names,
+                       const int64_t* param_values, int n_params);
+
+/* ---- one execution (replaces Interpreter<CudaBackend>::run) -------------- */
+bsz_run* bsz_run_create(bsz_program* prog, int64_t bitlength, int mode);
+void bsz_run_free(bsz_run* run);
+int bsz_set_param(bsz_run* run, const char* name, int64_t value);
+/* Binds an input stream.  index < 0: scalar input; index >= 0: element of an
+ * input array.  `words` holds n_words words on the host (on_device = 0, the
+ * copy is made on the context's stream) or on the device (on_device = 1, the
+ * buffer is copied so the caller keeps ownership).  Words beyond n_words are
+ * zero; words past ceil(bitlength/64) are ignored. */
+int bsz_bind_input(bsz_run* run, const char* name, int64_t index, const uint64_t* words,
+                   uint64_t n_words, int tail, int on_device);
+/* Binds a broadcast array (bsdata "_broadcast_pack"): element i is all-ones
+ * (-1) when ones[i] != 0, else zero. */
+int bsz_bind_broadcast(bsz_run* run, const char* name, const uint8_t* ones, int64_t count);
+/* Runs the program.  stats may be NULL. */
+int bsz_execute(bsz_run* run, bsz_stats* stats);
+/* Results.  For a stream output: copies ceil(bitlength/64) words (bits at and
+ * above the bitlength cleared, as the reference masks outputs) into host
+ * memory.  index < 0 for scalar outputs.  Returns nonzero if absent. */
+int bsz_get_stream(bsz_run* run, const char* name, int64_t index, uint64_t* host,
+                   uint64_t n_words);
+/* Device pointer of a stream output (valid until bsz_run_free). */
+int bsz_get_stream_device(bsz_run* run, const char* name, int64_t index,
+                          const uint64_t** dptr);
+int bsz_get_int(bsz_run* run, const char* name, int64_t* value);
+/* Indices present in an array output; returns the count (<= cap written),
+ * or -1 if the array does not exist. */
+int64_t bsz_array_indices(bsz_run* run, const char* name, int64_t* indices, int64_t cap);
+
+/* ---- whole-case driver (replaces run_case<64>, main.cu:23-207) ----------
+ * Runs `source` on every case of a .bsdata file (or, if bsdata_path is NULL,
+ * on the JSON input document `json_input`, the stdin form of main.cu) and
+ * returns the bsim_cuda JSON text (one object, or an array for multi-case
+ * files).  flags: bit 0 = --warmup, bit 1 = fused mode.  The returned string
+ * is owned by the library and valid until the next call on this thread. */
+const char* bsz_run_case_json(bsz_ctx* ctx, const char* source, const char* bsdata_path,
+                              const char* json_input, int flags);
+
+/* ---- per-op data plane on device pointers (CudaBackend op_*) -----------
+ * dst/a/b are device pointers to n_words words; `bitlength` is the logical
+ * length (bits at and above it are cleared by ~, + and <<).  All calls are
+ * asynchronous on the context's stream except popcount / is_nonzero, which
+ * return their result to the host. */
+int bsz_op_not(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, uint64_t n_words,
+               int64_t bitlength);
+int bsz_op_and(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b,
+               uint64_t n_words);
+int bsz_op_or(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b,
+              uint64_t n_words);
+int bsz_op_xor(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b,
+               uint64_t n_words);
+int bsz_op_andnot(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b,
+                  uint64_t n_words);
+int bsz_op_add(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b,
+               uint64_t n_words, int64_t bitlength);
+int bsz_op_shl(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, uint64_t k, uint64_t n_words,
+               int64_t bitlength);
+int bsz_op_shr(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, uint64_t k, uint64_t n_words,
+               int tail);
+int bsz_op_popcount(bsz_ctx* ctx, const uint64_t* a, uint64_t n_words, uint64_t* result);
+int bsz_op_is_nonzero(bsz_ctx* ctx, const uint64_t* a, uint64_t n_words, int* result);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BSZ_H_ */

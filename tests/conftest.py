@@ -62,3 +62,28 @@ def mask_outputs(out, ints, nbits):
 
 REFERENCE_TREE = os.environ.get("BSZ_REFERENCE_TREE", "/root/reference")
 has_reference = os.path.isdir(os.path.join(REFERENCE_TREE, "simulator", "pythonsim"))
+
+
+@pytest.fixture(scope="session")
+def ctx():
+    import bitstreamzoo_b200 as bz
+    c = bz.Context(0)
+    yield c
+    c.close()
+
+
+def run_golden_case(ctx, rec, mode):
+    """Runs a golden record through the C ABI; returns (masked outputs, op_count)."""
+    src, nbits, inputs, params, arrays = decode_case(rec)
+    r = ctx.run(src, nbits, inputs, params, arrays, mode=mode)
+    got = {}
+    mask = (1 << nbits) - 1
+    for k, v in rec["expected"].items():
+        if isinstance(v, dict) and "int" in v:
+            got[k] = r.int(k)
+        elif isinstance(v, dict):
+            idx = r.array_indices(k) or []
+            got[k] = {int(i): (r.stream_int(k, int(i)) & mask if int(i) in idx else 0) for i in v}
+        else:
+            got[k] = r.stream_int(k) & mask
+    return got, r.stats["op_count"], r
