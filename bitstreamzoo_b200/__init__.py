@@ -81,6 +81,16 @@ class Context:
     def sync(self):
         _lib.check(self.lib.bsz_sync(self.h))
 
+    def profile(self, enable: bool = True):
+        """Start (and reset) or stop per-kernel CUDA-event timing."""
+        _lib.check(self.lib.bsz_profile(self.h, 1 if enable else 0))
+
+    def profile_report(self) -> dict:
+        js = self.lib.bsz_profile_report(self.h)
+        if js is None:
+            raise BszError(_lib.last_error())
+        return json.loads(js.decode())
+
     def compile(self, source: str) -> "Program":
         return Program(self, source)
 

@@ -36,6 +36,8 @@ SIGNATURES = {
     "bsz_destroy": (None, [c_void_p]),
     "bsz_stream": (c_void_p, [c_void_p]),
     "bsz_sync": (ctypes.c_int, [c_void_p]),
+    "bsz_profile": (ctypes.c_int, [c_void_p, ctypes.c_int]),
+    "bsz_profile_report": (ctypes.c_char_p, [c_void_p]),
     "bsz_compile": (c_void_p, [c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "bsz_program_free": (None, [c_void_p]),
     "bsz_static_ops": (ctypes.c_int64, [c_void_p, ctypes.POINTER(ctypes.c_char_p), i64p, ctypes.c_int]),

@@ -13,14 +13,30 @@
 #include "frontend.h"
 #include "io.h"
 
+// Lifetimes: runs keep their program alive and programs keep their context
+// alive, so the handles may be freed in any order.
 struct bsz_ctx {
   std::unique_ptr<bsz::Device> dev;
+  int refs = 1;
 };
 
 struct bsz_program {
   bsz_ctx* ctx;
   std::unique_ptr<bsz::Program> prog;
+  int refs = 1;
 };
+
+static void ctx_unref(bsz_ctx* c) {
+  if (c && --c->refs == 0) delete c;
+}
+
+static void prog_unref(bsz_program* p) {
+  if (p && --p->refs == 0) {
+    bsz_ctx* c = p->ctx;
+    delete p;
+    ctx_unref(c);
+  }
+}
 
 struct bsz_run {
   bsz_program* prog;
@@ -29,6 +45,10 @@ struct bsz_run {
   std::unique_ptr<bsz::Executor> ex;
   std::vector<std::pair<int, int64_t>> params;
   bool done = false;
+  ~bsz_run() {
+    ex.reset();
+    prog_unref(prog);
+  }
 };
 
 namespace {
@@ -60,6 +80,18 @@ bsz::Executor& executor(bsz_run* r) {
   return *r->ex;
 }
 
+// Declared input name (or -1): inputs the program does not declare are
+// ignored, as both reference executors load only declared inputs
+// (interpreter.py:232-238, interpreter.inl:288-312).
+int input_id(bsz_run* r, const char* name) {
+  const bsz::Program& p = *r->prog->prog;
+  int id = p.find(name ? name : "");
+  if (id < 0) return -1;
+  for (int x : p.inputs)
+    if (x == id) return id;
+  return -1;
+}
+
 int name_id(bsz_run* r, const char* name) {
   int id = r->prog->prog->find(name ? name : "");
   if (id < 0) throw std::invalid_argument(std::string("unknown name: ") + (name ? name : "(null)"));
@@ -84,9 +116,21 @@ bsz_ctx* bsz_create(int device) {
   return c;
 }
 
-void bsz_destroy(bsz_ctx* ctx) { delete ctx; }
+void bsz_destroy(bsz_ctx* ctx) { ctx_unref(ctx); }
 
 void* bsz_stream(bsz_ctx* ctx) { return ctx ? static_cast<void*>(ctx->dev->stream()) : nullptr; }
+
+int bsz_profile(bsz_ctx* ctx, int enable) {
+  return guard([&] {
+    ctx->dev->prof_reset();
+    ctx->dev->profiling = enable != 0;
+  });
+}
+
+const char* bsz_profile_report(bsz_ctx* ctx) {
+  int rc = guard([&] { g_json = ctx->dev->prof_report(); });
+  return rc ? nullptr : g_json.c_str();
+}
 
 int bsz_sync(bsz_ctx* ctx) {
   return guard([&] {
@@ -102,13 +146,14 @@ bsz_program* bsz_compile(bsz_ctx* ctx, const char* source, size_t len) {
         auto prog = std::make_unique<bsz_program>();
         prog->ctx = ctx;
         prog->prog = bsz::parse_program(std::string(source, len));
+        if (ctx) ++ctx->refs;
         p = prog.release();
       }))
     return nullptr;
   return p;
 }
 
-void bsz_program_free(bsz_program* prog) { delete prog; }
+void bsz_program_free(bsz_program* prog) { prog_unref(prog); }
 
 int64_t bsz_static_ops(bsz_program* prog, const char* const* names, const int64_t* values, int n) {
   std::unordered_map<std::string, int64_t> params;
@@ -123,7 +168,13 @@ bsz_run* bsz_run_create(bsz_program* prog, int64_t bitlength, int mode) {
         run->prog = prog;
         run->bitlength = bitlength;
         run->mode = mode;
-        executor(run.get());
+        ++prog->refs;
+        try {
+          executor(run.get());
+        } catch (...) {
+          run->ex.reset();
+          throw;
+        }
         r = run.release();
       }))
     return nullptr;
@@ -143,8 +194,19 @@ int bsz_bind_input(bsz_run* run, const char* name, int64_t index, const uint64_t
                    uint64_t n_words, int tail, int on_device) {
   return guard([&] {
     bsz::Device& dev = *run->prog->ctx->dev;
-    const int id = name_id(run, name);
+    const int id = input_id(run, name);
+    if (id < 0) return;
     const int64_t nw = words_of(run->bitlength);
+    if (on_device == 2) {   // borrowed device buffer: no copy, caller keeps it alive
+      if (static_cast<int64_t>(n_words) < nw)
+        throw std::invalid_argument("borrowed input shorter than ceil(bitlength/64) words");
+      auto b = std::make_shared<bsz::DevStream>();
+      b->p = const_cast<uint64_t*>(words);
+      b->n_words = nw;
+      if (index < 0) executor(run).bind_input(id, b, tail ? 1 : 0, false);
+      else executor(run).bind_input_array(id, index, b, tail ? 1 : 0, false);
+      return;
+    }
     bsz::BufRef b = dev.alloc_stream(nw);
     const int64_t have = std::min<int64_t>(static_cast<int64_t>(n_words), nw);
     if (have > 0)
@@ -170,9 +232,11 @@ int bsz_bind_input(bsz_run* run, const char* name, int64_t index, const uint64_t
 
 int bsz_bind_broadcast(bsz_run* run, const char* name, const uint8_t* ones, int64_t count) {
   return guard([&] {
+    const int id = input_id(run, name);
+    if (id < 0) return;
     std::vector<uint8_t> v(ones, ones + count);
     for (auto& x : v) x = x ? 1 : 0;
-    executor(run).bind_broadcast(name_id(run, name), v);
+    executor(run).bind_broadcast(id, v);
   });
 }
 

@@ -2,6 +2,7 @@
 #include "device.h"
 
 #include <algorithm>
+#include <cstdio>
 
 namespace bsz {
 
@@ -128,6 +129,59 @@ uint32_t Device::take_error() {
 void Device::sync() {
   BSZ_CUDA(cudaStreamSynchronize(stream_));
   BSZ_CUDA(cudaGetLastError());
+}
+
+cudaEvent_t Device::prof_event() {
+  if (!prof_pool_.empty()) {
+    cudaEvent_t e = prof_pool_.back();
+    prof_pool_.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  BSZ_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+cudaEvent_t Device::prof_begin() {
+  cudaEvent_t e = prof_event();
+  BSZ_CUDA(cudaEventRecord(e, stream_));
+  return e;
+}
+
+void Device::prof_end(const char* name, cudaEvent_t begin) {
+  cudaEvent_t e = prof_event();
+  BSZ_CUDA(cudaEventRecord(e, stream_));
+  prof_pending_.push_back({name, begin, e});
+  if (prof_pending_.size() > 4096) prof_report();   // resolve in batches
+}
+
+std::string Device::prof_report() {
+  BSZ_CUDA(cudaStreamSynchronize(stream_));
+  for (auto& r : prof_pending_) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    auto& t = prof_totals_[r.name];
+    t.first += 1;
+    t.second += ms;
+    prof_pool_.push_back(r.a);
+    prof_pool_.push_back(r.b);
+  }
+  prof_pending_.clear();
+  std::string js = "{";
+  bool first = true;
+  for (auto& kv : prof_totals_) {
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "%s\"%s\":{\"launches\":%lld,\"ms\":%.6f}", first ? "" : ",",
+                  kv.first.c_str(), static_cast<long long>(kv.second.first), kv.second.second);
+    js += buf;
+    first = false;
+  }
+  return js + "}";
+}
+
+void Device::prof_reset() {
+  prof_report();
+  prof_totals_.clear();
 }
 
 }  // namespace bsz

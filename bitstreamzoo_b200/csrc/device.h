@@ -79,6 +79,13 @@ class Device {
   // Untyped device scratch (cached; grows).
   void* scratch(size_t bytes);
 
+  // Per-kernel CUDA-event timing on this device's stream (off by default).
+  bool profiling = false;
+  cudaEvent_t prof_begin();
+  void prof_end(const char* name, cudaEvent_t begin);
+  std::string prof_report();   // synchronizes; JSON {name: {launches, ms}}
+  void prof_reset();
+
  private:
   int ordinal_;
   int sm_count_ = 148;
@@ -91,6 +98,24 @@ class Device {
   void* d_scratch_ = nullptr;
   size_t scratch_cap_ = 0;
   void* raw_alloc(size_t bytes);
+  struct ProfRec { const char* name; cudaEvent_t a, b; };
+  std::vector<ProfRec> prof_pending_;
+  std::vector<cudaEvent_t> prof_pool_;
+  std::map<std::string, std::pair<int64_t, double>> prof_totals_;
+  cudaEvent_t prof_event();
+};
+
+// Records CUDA events around one launch when the device is profiling.
+struct ProfScope {
+  Device& d;
+  const char* name;
+  cudaEvent_t a = nullptr;
+  ProfScope(Device& dev, const char* n) : d(dev), name(n) {
+    if (d.profiling) a = d.prof_begin();
+  }
+  ~ProfScope() {
+    if (a) d.prof_end(name, a);
+  }
 };
 
 // ---------------------------------------------------------------------------

@@ -108,6 +108,8 @@ template <int OP>
 void launch_map(Device& dev, uint64_t* d, const uint64_t* a, const uint64_t* b, int64_t n,
                 uint64_t last_mask) {
   if (n <= 0) return;
+  static const char* names[] = {"k_and", "k_or", "k_xor", "k_andnot", "k_not"};
+  ProfScope prof(dev, names[OP]);
   const bool vec = aligned16(d) && aligned16(a) && (OP == 4 || aligned16(b));
   if (vec) {
     int64_t nvec = (n - 1) / 2;
@@ -379,6 +381,7 @@ void launch_shl(Device& dev, uint64_t* d, const uint64_t* a, int64_t k, int64_t 
   int64_t ws = std::min<int64_t>(k / 64, n + 1);
   int bs = static_cast<int>(k % 64);
   int grid = grid_for(dev, n, kThreads * kUnroll);
+  ProfScope prof(dev, "k_shl");
   k_shl<<<grid, kThreads, 0, dev.stream()>>>(d, a, ws, bs, n, last_mask);
   check_launch();
   ++dev.n_launches;
@@ -389,6 +392,7 @@ void launch_shr(Device& dev, uint64_t* d, const uint64_t* a, int64_t k, int64_t 
   int64_t ws = std::min<int64_t>(k / 64, n + 1);
   int bs = static_cast<int>(k % 64);
   int grid = grid_for(dev, n, kThreads * kUnroll);
+  ProfScope prof(dev, "k_shr");
   k_shr<<<grid, kThreads, 0, dev.stream()>>>(d, a, ws, bs, n, fill);
   check_launch();
   ++dev.n_launches;
@@ -401,6 +405,7 @@ void launch_add_with_state(Device& dev, uint64_t* d, const uint64_t* a, const ui
   if (n <= 0) return;
   int64_t tiles = (n + kAddTile - 1) / kAddTile;
   if (tiles > 0x7fffffff) throw std::invalid_argument("launch_add: stream too long");
+  ProfScope prof(dev, "k_add");
   k_add<<<static_cast<unsigned>(tiles), kAddWarps * 32, 0, dev.stream()>>>(
       d, a, b, n, last_mask, state, dev.error_word());
   check_launch();
@@ -418,6 +423,7 @@ void launch_popcount(Device& dev, const uint64_t* a, int64_t n, unsigned long lo
   if (n <= 0) return;
   int vec = aligned16(a) ? 1 : 0;
   int grid = grid_for(dev, vec ? std::max<int64_t>(n / 2, 1) : n, kThreads * (vec ? kUnroll : 1));
+  ProfScope prof(dev, "k_popcount");
   k_popcount<<<grid, kThreads, 0, dev.stream()>>>(a, n, slot, vec);
   check_launch();
   ++dev.n_launches;
@@ -426,6 +432,7 @@ void launch_popcount(Device& dev, const uint64_t* a, int64_t n, unsigned long lo
 void launch_any(Device& dev, const uint64_t* a, int64_t n, unsigned int* flag) {
   if (n <= 0) return;
   int grid = grid_for(dev, n, kThreads * 4);
+  ProfScope prof(dev, "k_any");
   k_any<<<grid, kThreads, 0, dev.stream()>>>(a, n, flag);
   check_launch();
   ++dev.n_launches;
@@ -434,6 +441,7 @@ void launch_any(Device& dev, const uint64_t* a, int64_t n, unsigned int* flag) {
 void launch_fill(Device& dev, uint64_t* d, int64_t n, uint64_t value, uint64_t last_value) {
   if (n <= 0) return;
   int grid = grid_for(dev, n, kThreads * 4);
+  ProfScope prof(dev, "k_fill");
   k_fill<<<grid, kThreads, 0, dev.stream()>>>(d, n, value, last_value);
   check_launch();
   ++dev.n_launches;

@@ -64,6 +64,11 @@ void bsz_destroy(bsz_ctx* ctx);
 /* The context's cudaStream_t, as void*. */
 void* bsz_stream(bsz_ctx* ctx);
 int bsz_sync(bsz_ctx* ctx);
+/* Per-kernel timing with CUDA events on the context's stream: enable != 0
+ * starts (and resets) it.  bsz_profile_report() synchronizes and returns
+ * JSON {"kernel name": {"launches": n, "ms": total}}, owned by the library. */
+int bsz_profile(bsz_ctx* ctx, int enable);
+const char* bsz_profile_report(bsz_ctx* ctx);
 
 /* ---- programs (replaces bs::parse, simulator/csim/src/parser.cpp:451-457) */
 /* Parses and validates DSL source.  NULL on ParseError / ThreeAddrError. */
@@ -80,8 +85,11 @@ int bsz_set_param(bsz_run* run, const char* name, int64_t value);
 /* Binds an input stream.  index < 0: scalar input; index >= 0: element of an
  * input array.  `words` holds n_words words on the host (on_device = 0, the
  * copy is made on the context's stream) or on the device (on_device = 1, the
- * buffer is copied so the caller keeps ownership).  Words beyond n_words are
- * zero; words past ceil(bitlength/64) are ignored. */
+ * buffer is copied so the caller keeps ownership; on_device = 2, the device
+ * buffer is borrowed without a copy and must stay valid and unchanged until
+ * bsz_run_free).  Words beyond n_words are zero (or all ones when tail = 1);
+ * words past ceil(bitlength/64) are ignored.  Names the program does not
+ * declare as inputs are ignored, as the reference executors ignore them. */
 int bsz_bind_input(bsz_run* run, const char* name, int64_t index, const uint64_t* words,
                    uint64_t n_words, int tail, int on_device);
 /* Binds a broadcast array (bsdata "_broadcast_pack"): element i is all-ones
