@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""Benchmark: input GB/s and HBM-roofline fraction of the B200 bitstream
+executor on the long-stream workload (two 2^32-bit streams: A + B,
+A << {1, 63, 64, 1000}, A ^ B, A & ~B and the popcount of each), fused vs
+plain per-op, bit-exact.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--nbits BITS] [--mode fused|plain]
+
+One step = one pass of the program over one pair of streams.  ``value`` is
+the input GB/s of the fused form with inputs resident in HBM (device time,
+CUDA events on the executor's stream, max over ranks); ``e2e`` is the same
+metric through the C ABI with pinned host inputs copied in and every output
+stream + popcount copied out inside the timed region.  Inputs (1 GiB per
+rank) are larger than L2, so no L2 flush is needed between steps.
+
+``--impl reference`` times the reference's own CPU executor (bsim, built from
+the reference sources by oracle/Makefile, AVX-512 + OpenMP on all host cores)
+on a bounded sample of the same program; rank 0 alone runs it.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+WORKLOAD = "long_streams"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nbits", type=int, default=1 << 32)
+    ap.add_argument("--mode", default="fused", choices=["fused", "plain"])
+    ap.add_argument("--cpu-sample-bits", type=int, default=1 << 28)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU side --
+
+def cpu_baseline(nbits: int, reps: int, warm: int = 1):
+    """Reference CPU executor (bsim, AVX-512 + OpenMP, all host threads) on a
+    bounded sample of the workload.  Falls back to the C port of the oracle
+    when the reference binary was not built."""
+    from bitstreamzoo_b200 import workloads as wl
+    from bitstreamzoo_b200.bsdata import write_bsdata
+    threads = os.cpu_count() or 1
+    bsim = os.path.join(ROOT, "oracle", "_ref", "bsim")
+    inputs = wl.long_streams_inputs(nbits, seed=99)
+    in_bytes = 2 * nbits // 8
+    if os.path.exists(bsim):
+        with tempfile.TemporaryDirectory() as td:
+            prog = os.path.join(td, "long_streams.bs")
+            with open(prog, "w") as f:
+                f.write(wl.long_streams_src())
+            data = os.path.join(td, "in.bsdata")
+            write_bsdata(data, nbits, inputs)
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads),
+                       GLIBC_TUNABLES="glibc.cpu.x86_rep_stosb_threshold=2000000000")
+            times = []
+            for i in range(warm + reps):
+                out = os.path.join(td, "out.json")
+                with open(out, "w") as fo:
+                    r = subprocess.run([bsim, prog, "--backend", "simd_omp", "--reuse-mem",
+                                        "--input", data], stdout=fo, stderr=subprocess.PIPE,
+                                       env=env, timeout=600)
+                if r.returncode != 0:
+                    raise RuntimeError(r.stderr.decode()[-500:])
+                with open(out, "rb") as fi:
+                    head = fi.read(4096).decode(errors="replace")
+                ms = float(head.split('"exec_ms":', 1)[1].split(",", 1)[0])
+                if i >= warm:
+                    times.append(ms)
+        ms = statistics.median(times)
+        return {"value": in_bytes / (ms * 1e-3) / 1e9, "unit": "GB/s", "cores": threads,
+                "kind": "reference", "ms_per_step": ms,
+                "sample": (f"long_streams program at {nbits} bits (1/{(1 << 32) // nbits} of the "
+                           f"2^32-bit workload), bsim --backend simd_omp, OMP_NUM_THREADS={threads}, "
+                           f"median exec_ms of {len(times)} runs")}
+    # C port of the oracle
+    from oracle import cwords, pyoracle
+    prog = pyoracle.parse(wl.long_streams_src())
+    times = []
+    for i in range(warm + reps):
+        t0 = time.perf_counter()
+        cwords.run_straight_line(prog, nbits, inputs)
+        if i >= warm:
+            times.append((time.perf_counter() - t0) * 1e3)
+    ms = statistics.median(times)
+    return {"value": in_bytes / (ms * 1e-3) / 1e9, "unit": "GB/s",
+            "cores": cwords.lib().o_num_threads(), "kind": "port", "ms_per_step": ms,
+            "sample": f"long_streams program at {nbits} bits, oracle C port, median of {len(times)}"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 5))
+    cb = cpu_baseline(args.cpu_sample_bits, steps, warm=min(1, args.warmup))
+    line = {"metric": "input GB/s (long-stream primitives, bit-exact)", "value": cb["value"],
+            "unit": "GB/s", "n_gpus": 0, "steps": steps, "warmup": min(1, args.warmup),
+            "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"{WORKLOAD}: A+B, A<<{{1,63,64,1000}}, A^B, A&~B, popcounts; "
+                                   f"sample {args.cpu_sample_bits} bits of 2^32"},
+            "cpu_baseline": {k: cb[k] for k in ("kind", "cores", "sample", "value", "unit")},
+            "e2e": {"value": cb["value"], "unit": "GB/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU side --
+
+# Algorithmic bytes per launch for each kernel, as a function of N (bits).
+def kernel_bytes(name: str, nbits: int, n_out_streams: int = 7, n_pops: int = 7) -> float:
+    s = nbits / 8
+    table = {"k_and": 3 * s, "k_or": 3 * s, "k_xor": 3 * s, "k_andnot": 3 * s, "k_not": 2 * s,
+             "k_shl": 2 * s, "k_shr": 2 * s, "k_add": 3 * s, "k_popcount": s + 8, "k_fill": s,
+             "k_any": s}
+    if name.startswith("fused"):
+        return 2 * s + n_out_streams * s + 8 * n_pops
+    return table.get(name, float("nan"))
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    import bitstreamzoo_b200 as bz
+    from bitstreamzoo_b200 import workloads as wl
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    hbm, hbm_src = peaks()
+    nbits = args.nbits
+    nw = wl.n_words(nbits)
+    ctx = bz.Context(local)
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    prog = ctx.compile(wl.long_streams_src())
+    host = wl.long_streams_inputs(nbits, seed=20261204 + rank)
+    dA = torch.from_numpy(host["A"].view(np.int64)).to(dev)
+    dB = torch.from_numpy(host["B"].view(np.int64)).to(dev)
+    torch.cuda.synchronize()
+    in_bytes = 2 * nbits // 8
+    mode_of = {"fused": bz.MODE_FUSED, "plain": bz.MODE_PLAIN}
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def step(mode):
+        r = prog.run(nbits, mode)
+        r.bind("A", ("borrow", dA.data_ptr(), nw))
+        r.bind("B", ("borrow", dB.data_ptr(), nw))
+        st = r.execute()
+        pops = {n: r.int(n) for n in wl.LONG_OUTPUT_INTS}
+        del r
+        return st, pops
+
+    forms = {}
+    order = [args.mode] + [m for m in ("fused", "plain") if m != args.mode]
+    for name in order:
+        mode = mode_of[name]
+        try:
+            for _ in range(args.warmup):
+                st, pops = step(mode)
+        except bz.BszError as e:
+            forms[name] = {"unavailable": str(e)[:200]}
+            continue
+        barrier()
+        ctx.profile(True)
+        clocks = Clocks(local)
+        clocks.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        launches = 0
+        for _ in range(args.steps):
+            st, pops = step(mode)
+            launches += st["n_kernel_launches"]
+        e1.record(ext)
+        e1.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        ck = clocks.stop()
+        prof = ctx.profile_report()
+        ctx.profile(False)
+        ms_max = max_over_ranks(ms)
+        forms[name] = {"ms": ms_max, "launches": launches, "profile": prof, "clocks": ck,
+                       "pops": pops,
+                       "value": world * in_bytes * args.steps / (ms_max * 1e-3) / 1e9}
+
+    # sanity (bit-exact popcounts that are cheap to check on the host)
+    ref_px = int(np.bitwise_count(host["A"] ^ host["B"]).sum())
+    ref_pl64 = int(np.bitwise_count(host["A"][:-1]).sum())
+    for name, f in forms.items():
+        if "pops" in f:
+            f["check"] = (f["pops"]["px"] == ref_px and f["pops"]["pl64"] == ref_pl64)
+
+    # end to end through the C ABI: pinned host in, all outputs out
+    e2e = None
+    main = forms.get(args.mode, {})
+    if not args.no_e2e and "ms" in main:
+        mode = mode_of[args.mode]
+        pA = torch.from_numpy(host["A"].view(np.int64)).pin_memory()
+        pB = torch.from_numpy(host["B"].view(np.int64)).pin_memory()
+        outs = {n: torch.empty(nw, dtype=torch.int64).pin_memory() for n in wl.LONG_OUTPUT_STREAMS}
+        a_np, b_np = pA.numpy().view(np.uint64), pB.numpy().view(np.uint64)
+        o_np = {n: t.numpy().view(np.uint64) for n, t in outs.items()}
+
+        def e2e_step():
+            r = prog.run(nbits, mode)
+            r.bind("A", a_np)
+            r.bind("B", b_np)
+            r.execute()
+            for n in wl.LONG_OUTPUT_STREAMS:
+                bz._lib.check(r.lib.bsz_get_stream(r.h, n.encode(), -1, o_np[n].ctypes.data, nw))
+            pops = [r.int(n) for n in wl.LONG_OUTPUT_INTS]
+            del r
+            return pops
+
+        for _ in range(max(1, min(args.warmup, 2))):
+            e2e_step()
+        barrier()
+        k = max(1, min(args.steps, 5))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(ext)
+        for _ in range(k):
+            e2e_step()
+        e1.record(ext)
+        e1.synchronize()
+        wall = (time.perf_counter() - t0) * 1e3
+        barrier()
+        ms = max_over_ranks(max(e0.elapsed_time(e1), wall))
+        e2e = {"value": world * in_bytes * k / (ms * 1e-3) / 1e9, "unit": "GB/s",
+               "h2d_bytes_per_step": in_bytes,
+               "d2h_bytes_per_step": len(wl.LONG_OUTPUT_STREAMS) * nw * 8 + 8 * len(wl.LONG_OUTPUT_INTS),
+               "steps": k, "ms_per_step": ms / k}
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_baseline(args.cpu_sample_bits, 3)
+        except Exception as e:  # noqa: BLE001
+            cb = {"unavailable": str(e)[:200]}
+
+    if rank == 0:
+        main = forms.get(args.mode, {})
+        value = main.get("value")
+        prof = main.get("profile", {})
+        roof = None
+        if prof:
+            top = max(prof.items(), key=lambda kv: kv[1]["ms"])
+            kname, kv = top
+            per_launch_ms = kv["ms"] / max(1, kv["launches"])
+            bytes_launch = kernel_bytes(kname, nbits)
+            achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
+            traffic = None
+            tpath = os.path.join(ROOT, "profiles", "traffic.json")
+            if os.path.exists(tpath):
+                with open(tpath) as f:
+                    traffic = json.load(f).get(kname)
+            roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
+                    "peak_source": hbm_src, "unit": "GB/s", "frac": achieved / hbm,
+                    "traffic": traffic, "bytes_per_launch": bytes_launch,
+                    "launch_ms": per_launch_ms,
+                    "kernel_share": kv["ms"] / max(1e-9, sum(x["ms"] for x in prof.values()))}
+        step_bytes = in_bytes + 7 * nbits // 8 + 56
+        line = {
+            "metric": "input GB/s (long-stream primitives, bit-exact)",
+            "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": main.get("ms", float("nan")) / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded: A ~ Bernoulli(1/2), B ones with zeros at p=2^-20)",
+            "config": {"workload": (f"{WORKLOAD}: two {nbits}-bit streams per GPU; A+B, "
+                                    "A<<{1,63,64,1000}, A^B, A&~B + 7 popcounts"),
+                       "form": args.mode, "bits_per_stream": nbits,
+                       "l2": "inputs (1 GiB/GPU) larger than L2; no flush needed",
+                       "parallelism": f"replicas x{world} (independent stream pairs)"},
+            "hbm_frac_step": (step_bytes * args.steps / (main.get("ms", float("nan")) * 1e-3) / 1e9) / hbm
+            if main.get("ms") else None,
+            "roofline": roof,
+            "cpu_baseline": cb,
+            "e2e": e2e,
+            "gpu_launches": main.get("launches"),
+            "clocks": main.get("clocks"),
+            "forms": {k: {kk: vv for kk, vv in v.items() if kk not in ("pops",)} for k, v in forms.items()},
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

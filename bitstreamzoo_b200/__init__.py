@@ -188,12 +188,14 @@ class Run:
         _lib.check(self.lib.bsz_set_param(self.h, name.encode(), int(value)))
 
     def bind(self, name: str, value, index: int = -1, tail: int = 0):
-        """Bind a Python int, a numpy uint64 array, or a device pointer
-        (``("device", ptr, n_words)``)."""
-        if isinstance(value, tuple) and value and value[0] == "device":
-            _, ptr, nw = value[:3]
+        """Bind a Python int, a numpy uint64 array, or a device pointer:
+        ``("device", ptr, n_words)`` copies it, ``("borrow", ptr, n_words)``
+        uses it in place (it must outlive this run)."""
+        if isinstance(value, tuple) and value and value[0] in ("device", "borrow"):
+            kind, ptr, nw = value[:3]
             t = value[3] if len(value) > 3 else tail
-            _lib.check(self.lib.bsz_bind_input(self.h, name.encode(), index, ptr, nw, t, 1))
+            flag = 1 if kind == "device" else 2
+            _lib.check(self.lib.bsz_bind_input(self.h, name.encode(), index, ptr, nw, t, flag))
             return
         if isinstance(value, np.ndarray):
             w = np.ascontiguousarray(value, dtype=np.uint64)

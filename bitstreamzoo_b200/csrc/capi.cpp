@@ -268,6 +268,8 @@ int bsz_execute(bsz_run* run, bsz_stats* stats) {
       stats->max_live = ex.max_live_buffers;
       stats->kernel_ms = ms;
       stats->compile_ms = ex.compile_ms;
+      stats->n_fused_launches = ex.fused_launches();
+      stats->n_fused_fallbacks = ex.fused_fallbacks();
     }
   });
 }

@@ -58,6 +58,9 @@ Executor::~Executor() {
   if (d_slots_) cudaFree(d_slots_);
 }
 
+int64_t Executor::fused_launches() const { return fused_ ? fused_->launches : 0; }
+int64_t Executor::fused_fallbacks() const { return fused_ ? fused_->fallbacks : 0; }
+
 void Executor::set_param(int name, int64_t v) {
   if (name < 0) return;
   ints_[name] = IntV{v, -1};

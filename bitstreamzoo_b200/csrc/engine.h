@@ -97,6 +97,8 @@ class Executor {
   int64_t n_syncs = 0;
   int64_t max_live_buffers = 0;
   double compile_ms = 0.0;
+  int64_t fused_launches() const;
+  int64_t fused_fallbacks() const;
 
  private:
   struct IntV { int64_t v = 0; int32_t e = -1; };

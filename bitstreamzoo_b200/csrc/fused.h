@@ -22,6 +22,9 @@ class FusedBackend {
   void run(std::vector<Node>& nodes, const Segment& seg, int64_t N, int64_t nw,
            unsigned long long* d_slots, double* compile_ms);
 
+  int64_t fallbacks = 0;   // parts re-run with the plain kernels (speculation unproven)
+  int64_t launches = 0;    // fused kernels launched
+
   struct Impl;
 
  private:

@@ -51,6 +51,8 @@ typedef struct bsz_stats {
   int64_t max_live;          /* peak number of live stream buffers */
   double kernel_ms;          /* CUDA-event time of the execution */
   double compile_ms;         /* time spent generating/compiling fused kernels */
+  int64_t n_fused_launches;  /* generated segment kernels launched */
+  int64_t n_fused_fallbacks; /* segment parts re-run per-op because speculation was unproven */
 } bsz_stats;
 
 /* ---- library ---------------------------------------------------------- */

@@ -1,0 +1,116 @@
+"""Fused (generated persistent kernel) path at sizes where many warps share a
+stream, so every warp's start state comes from speculative warm-up.
+
+Each case runs through the C ABI in plain and fused form and is compared
+word for word with the word-level C oracle: the long-stream primitives
+(add with long carry runs, shifts by 1/63/64/1000), regex-shaped DAGs with
+chained additions and shifted temporaries, right shifts (which cut the
+segment), and an addition whose carry never resolves (x + ~x), where
+speculation cannot be proven and the exact per-op re-run must take over.
+"""
+
+import random
+
+import numpy as np
+import pytest
+
+import bitstreamzoo_b200 as bz
+from bitstreamzoo_b200 import workloads as wl
+from oracle import cwords, pyoracle
+import progen
+
+
+def run_both(ctx, src, nbits, inputs):
+    prog = pyoracle.parse(src)
+    ref_out, ref_pops = cwords.run_straight_line(prog, nbits, inputs)
+    results = {}
+    for mode in (bz.MODE_PLAIN, bz.MODE_FUSED):
+        r = ctx.run(src, nbits, inputs, mode=mode)
+        for name, words in ref_out.items():
+            got = r.stream(name)
+            exp = words.copy()
+            exp[-1] &= np.uint64(bz_mask(nbits))
+            if not np.array_equal(got, exp):
+                bad = int(np.argmax(got != exp))
+                raise AssertionError(f"mode {mode} output {name}: first bad word {bad} of {got.size}")
+        for name, v in ref_pops.items():
+            assert r.int(name) == v, (mode, name)
+        results[mode] = r.stats
+    return results
+
+
+def bz_mask(nbits):
+    r = nbits % 64
+    return ((1 << r) - 1) if r else (1 << 64) - 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nbits", [(1 << 22) + 37, 1 << 24])
+def test_long_streams(ctx, nbits):
+    inputs = wl.long_streams_inputs(nbits, seed=nbits)
+    st = run_both(ctx, wl.long_streams_src(), nbits, inputs)
+    assert st[bz.MODE_FUSED]["n_fused_launches"] >= 1
+
+
+@pytest.mark.gpu
+def test_matchstar(ctx):
+    nbits = (1 << 22) + 5
+    inputs = wl.matchstar_inputs(nbits, seed=3)
+    run_both(ctx, wl.MATCHSTAR_SRC, nbits, inputs)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_ops,seed", [(300, 1), (300, 2), (2000, 3)])
+def test_regex_dag(ctx, n_ops, seed):
+    nbits = (1 << 20) + 64 * 3 + 11
+    src = wl.regex_dag_src(n_ops=n_ops, seed=seed)
+    inputs = wl.regex_dag_inputs(nbits, seed=seed)
+    run_both(ctx, src, nbits, inputs)
+
+
+@pytest.mark.gpu
+def test_chained_adds_and_shifted_temporaries(ctx):
+    src = ("input stream a\ninput stream b\ninput stream c\noutput stream r\noutput stream q\n"
+           "output int n\n"
+           "stream s1 = a + b\nstream t1 = s1 << 1\nstream s2 = t1 + c\nstream t2 = s2 << 700\n"
+           "stream m = t2 & a\nstream s3 = m + s2\nstream t3 = s3 << 64\nr = t3 ^ s1\n"
+           "stream u = s3 >> 3\nstream v = u + a\nq = v << 5\nn = popcount(q)\n")
+    nbits = (1 << 21) + 17
+    rng = np.random.default_rng(9)
+    inputs = {k: wl.random_words(rng, nbits) for k in "abc"}
+    run_both(ctx, src, nbits, inputs)
+
+
+@pytest.mark.gpu
+def test_unresolvable_carry_falls_back_exactly(ctx):
+    src = ("input stream x\ninput stream z\noutput stream r\noutput int n\n"
+           "stream y = ~x\nstream s = x + y\nstream t = s << 1\nr = t + z\nn = popcount(r)\n")
+    nbits = 1 << 22
+    rng = np.random.default_rng(4)
+    inputs = {"x": wl.random_words(rng, nbits), "z": wl.random_words(rng, nbits)}
+    st = run_both(ctx, src, nbits, inputs)
+    assert st[bz.MODE_FUSED]["n_fused_fallbacks"] >= 1
+
+
+@pytest.mark.gpu
+def test_random_straight_line_programs_fused_matches_plain_and_oracle(ctx):
+    for seed in range(12):
+        rng = random.Random(seed)
+        nbits = rng.choice([64 * 2048 + 3, 64 * 4096, 100000])
+        src, meta = progen.random_program(rng, n_stmts=40, allow_ctrl=False)
+        inputs = {n: progen.rand_stream(rng, nbits) for n in meta["inputs"]}
+        arrays = {"arr_in": {i: progen.rand_stream(rng, nbits) for i in range(4)}}
+        try:
+            want, ops, _ = pyoracle.run_source(src, nbits, inputs, meta["params"], arrays)
+        except Exception:
+            continue
+        mask = (1 << nbits) - 1
+        for mode in (bz.MODE_PLAIN, bz.MODE_FUSED):
+            r = ctx.run(src, nbits, inputs, meta["params"], arrays, mode=mode)
+            assert r.stream_int("out0") & mask == want["out0"] & mask, (seed, mode)
+            assert r.stream_int("out1") & mask == want["out1"] & mask, (seed, mode)
+            for j in range(3):
+                exp = want["outa"].get(j, 0) & mask
+                assert r.stream_int("outa", j) & mask == exp, (seed, mode, j)
+            assert r.int("cnt") == want["cnt"], (seed, mode)
+            assert r.stats["op_count"] == ops
