@@ -65,8 +65,11 @@ def build(force: bool = False, verbose: bool = False) -> dict:
         objs = list(ex.map(lambda s: _compile(s, force, verbose), LIB_SOURCES))
         mains = list(ex.map(lambda s: _compile(s, force, verbose), MAIN_SOURCES))
     so = os.path.join(LIB, "libbsz.so")
-    link_libs = ["-L", os.path.join(CUDA_HOME, "lib64"), "-L", os.path.join(CUDA_HOME, "lib64", "stubs"),
-                 "-lnvrtc", "-lcuda", "-lcudart"]
+    # no -lcuda: driver entry points are resolved at run time (fused.cpp);
+    # the CUDA runtime is linked statically (the toolkit version it was built
+    # with), so whatever libcudart another library in the process loads does
+    # not matter.
+    link_libs = ["-L", os.path.join(CUDA_HOME, "lib64"), "-lnvrtc", "-cudart", "static"]
     if force or _newer(so, objs):
         cmd = [NVCC, *ARCH, "-shared", "-o", so, *objs, *link_libs,
                "-Xlinker", "-rpath", "-Xlinker", os.path.join(CUDA_HOME, "lib64")]

@@ -43,12 +43,47 @@
 namespace bsz {
 namespace {
 
+// Driver entry points are resolved at run time through the runtime API, so
+// the library has no link-time dependency on libcuda (it loads on hosts
+// without a driver, where only the front end is usable).
+struct Driver {
+  CUresult (*module_load_data)(CUmodule*, const void*) = nullptr;
+  CUresult (*module_get_function)(CUfunction*, CUmodule, const char*) = nullptr;
+  CUresult (*func_get_attribute)(int*, CUfunction_attribute, CUfunction) = nullptr;
+  CUresult (*launch_kernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
+                            unsigned, CUstream, void**, void**) = nullptr;
+  CUresult (*get_error_string)(CUresult, const char**) = nullptr;
+};
+
+template <class F>
+void resolve(const char* name, F& fn) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  cudaError_t e = cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q);
+  if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p)
+    throw CudaError(std::string("cannot resolve driver entry point ") + name);
+  fn = reinterpret_cast<F>(p);
+}
+
+const Driver& drv() {
+  static Driver d = [] {
+    Driver x;
+    resolve("cuModuleLoadData", x.module_load_data);
+    resolve("cuModuleGetFunction", x.module_get_function);
+    resolve("cuFuncGetAttribute", x.func_get_attribute);
+    resolve("cuLaunchKernel", x.launch_kernel);
+    resolve("cuGetErrorString", x.get_error_string);
+    return x;
+  }();
+  return d;
+}
+
 #define BSZ_CU(call)                                                              \
   do {                                                                            \
     CUresult r_ = (call);                                                         \
     if (r_ != CUDA_SUCCESS) {                                                     \
       const char* s_ = nullptr;                                                   \
-      cuGetErrorString(r_, &s_);                                                  \
+      drv().get_error_string(r_, &s_);                                            \
       throw CudaError(std::string(#call) + " failed: " + (s_ ? s_ : "?"));        \
     }                                                                             \
   } while (0)
@@ -401,9 +436,9 @@ Compiled compile_source(const std::string& src, double* compile_ms) {
   nvrtcGetCUBIN(prog, &cubin[0]);
   nvrtcDestroyProgram(&prog);
   Compiled c;
-  BSZ_CU(cuModuleLoadData(&c.mod, cubin.data()));
-  BSZ_CU(cuModuleGetFunction(&c.fn, c.mod, "bsz_fused"));
-  cuFuncGetAttribute(&c.n_regs, CU_FUNC_ATTRIBUTE_NUM_REGS, c.fn);
+  BSZ_CU(drv().module_load_data(&c.mod, cubin.data()));
+  BSZ_CU(drv().module_get_function(&c.fn, c.mod, "bsz_fused"));
+  drv().func_get_attribute(&c.n_regs, CU_FUNC_ATTRIBUTE_NUM_REGS, c.fn);
   if (compile_ms)
     *compile_ms += std::chrono::duration<double, std::milli>(std::chrono::high_resolution_clock::now() - t0).count();
   std::lock_guard<std::mutex> lk(g_cache_mu);
@@ -512,7 +547,7 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
     void* kparams[] = {args.data()};
     {
       ProfScope prof(dev, "fused");
-      BSZ_CU(cuLaunchKernel(c.fn, blocks, 1, 1, opt.fused_warps * 32, 1, 1, 0,
+      BSZ_CU(drv().launch_kernel(c.fn, blocks, 1, 1, opt.fused_warps * 32, 1, 1, 0,
                             reinterpret_cast<CUstream>(dev.stream()), kparams, nullptr));
     }
     ++dev.n_launches;
