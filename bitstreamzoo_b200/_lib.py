@@ -70,6 +70,8 @@ SIGNATURES = {
     "bsz_op_shr": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_uint64, ctypes.c_uint64,
                                   ctypes.c_int]),
     "bsz_op_popcount": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_uint64, u64p]),
+    "bsz_add_noalloc": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_uint64, ctypes.c_int64,
+                                       c_void_p]),
     "bsz_op_is_nonzero": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_uint64,
                                          ctypes.POINTER(ctypes.c_int)]),
 }

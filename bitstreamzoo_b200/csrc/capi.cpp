@@ -100,6 +100,10 @@ int name_id(bsz_run* r, const char* name) {
 
 }  // namespace
 
+namespace bsz {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace bsz
+
 extern "C" {
 
 const char* bsz_version(void) { return "bitstreamzoo_b200 0.1 (sm_100a)"; }

@@ -140,6 +140,10 @@ void launch_add(Device& dev, uint64_t* d, const uint64_t* a, const uint64_t* b, 
 void launch_add_with_state(Device& dev, uint64_t* d, const uint64_t* a, const uint64_t* b,
                            int64_t n, uint64_t last_mask, uint32_t* state);
 int64_t add_state_words(int64_t n);
+// The same carry-scan kernel on a caller's stream with caller-provided
+// look-back state (add_state_words(n) zeroed words) and error word.
+void launch_add_on_stream(cudaStream_t stream, uint64_t* d, const uint64_t* a, const uint64_t* b,
+                          int64_t n, uint64_t last_mask, uint32_t* state, uint32_t* err);
 void launch_popcount(Device& dev, const uint64_t* a, int64_t n,
                      unsigned long long* slot);
 void launch_any(Device& dev, const uint64_t* a, int64_t n, unsigned int* flag);

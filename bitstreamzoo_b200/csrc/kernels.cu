@@ -412,6 +412,14 @@ void launch_add_with_state(Device& dev, uint64_t* d, const uint64_t* a, const ui
   ++dev.n_launches;
 }
 
+void launch_add_on_stream(cudaStream_t stream, uint64_t* d, const uint64_t* a, const uint64_t* b,
+                          int64_t n, uint64_t last_mask, uint32_t* state, uint32_t* err) {
+  if (n <= 0) return;
+  int64_t tiles = (n + kAddTile - 1) / kAddTile;
+  k_add<<<static_cast<unsigned>(tiles), kAddWarps * 32, 0, stream>>>(d, a, b, n, last_mask, state, err);
+  check_launch();
+}
+
 void launch_add(Device& dev, uint64_t* d, const uint64_t* a, const uint64_t* b, int64_t n,
                 uint64_t last_mask) {
   if (n <= 0) return;

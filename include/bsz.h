@@ -145,6 +145,24 @@ int bsz_op_shr(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, uint64_t k, uint6
 int bsz_op_popcount(bsz_ctx* ctx, const uint64_t* a, uint64_t n_words, uint64_t* result);
 int bsz_op_is_nonzero(bsz_ctx* ctx, const uint64_t* a, uint64_t n_words, int* result);
 
+/* Stream addition that allocates no device memory (no counterpart in the
+ * reference).  For callers that cannot allocate GPU memory when they call:
+ * a serving process whose pool already holds almost all of HBM, a host
+ * application that passes its own buffers through FFI and owns every
+ * allocation, or a loop that cannot pay for the device-wide synchronisation
+ * of cudaMalloc/cudaFree.  Same result as bsz_op_add (dst = a + b with bits
+ * at and above `bitlength` cleared); no context is needed.  The look-back
+ * scratch is a fixed file-scope device array of about 129 KiB that every GPU
+ * loading the library keeps until exit, so n_words is limited to 2^26
+ * (streams of up to 2^32 bits); longer streams are rejected with an error.
+ * The first call on a device looks up that array's address (do it before
+ * any stream capture).  Every call reuses the same array, so calls that
+ * overlap on the GPU (different streams, or different host threads) race;
+ * serialize them.  Runs on `stream` (a cudaStream_t, NULL for the default
+ * stream) and returns when the addition has finished. */
+int bsz_add_noalloc(uint64_t* dst, const uint64_t* a, const uint64_t* b, uint64_t n_words,
+                    int64_t bitlength, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
