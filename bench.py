@@ -1,22 +1,26 @@
 #!/usr/bin/env python
 """Benchmark: input GB/s and HBM-roofline fraction of the B200 bitstream
-executor on the long-stream workload (two 2^32-bit streams: A + B,
-A << {1, 63, 64, 1000}, A ^ B, A & ~B and the popcount of each), fused vs
-plain per-op, bit-exact.
+executor, fused vs plain per-op, bit-exact.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--nbits BITS] [--mode fused|plain]
+                    [--workload long_streams|regex_dag|matchstar] [--nbits BITS]
+                    [--mode fused|plain]
 
-One step = one pass of the program over one pair of streams.  ``value`` is
-the input GB/s of the fused form with inputs resident in HBM (device time,
+Default workload (the one the headline metric is quoted on): two 2^32-bit
+streams per GPU, A + B, A << {1, 63, 64, 1000}, A ^ B, A & ~B and the popcount
+of each.  ``regex_dag`` is the 2,000-op regex-shaped DAG over 8 basis streams
+of 2^29 bits; ``matchstar`` the 2^24-bit MatchStar primitive.
+
+One step = one pass of the program over one set of input streams.  ``value``
+is the input GB/s of the fused form with inputs resident in HBM (device time,
 CUDA events on the executor's stream, max over ranks); ``e2e`` is the same
 metric through the C ABI with pinned host inputs copied in and every output
-stream + popcount copied out inside the timed region.  Inputs (1 GiB per
-rank) are larger than L2, so no L2 flush is needed between steps.
+stream + popcount copied out inside the timed region.  The default inputs
+(1 GiB per rank) are larger than L2, so no L2 flush is needed between steps.
 
 ``--impl reference`` times the reference's own CPU executor (bsim, built from
 the reference sources by oracle/Makefile, AVX-512 + OpenMP on all host cores)
-on a bounded sample of the same program; rank 0 alone runs it.
+on a bounded sample of the same workload; rank 0 alone runs it.
 """
 
 from __future__ import annotations
@@ -37,7 +41,6 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FALLBACK_HBM_GBS = 6650.0
-WORKLOAD = "long_streams"
 
 
 def parse_args():
@@ -46,12 +49,63 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--nbits", type=int, default=1 << 32)
+    ap.add_argument("--workload", default="long_streams", choices=["long_streams", "regex_dag", "matchstar"])
+    ap.add_argument("--nbits", type=int, default=0, help="bits per stream (default: the workload's)")
     ap.add_argument("--mode", default="fused", choices=["fused", "plain"])
-    ap.add_argument("--cpu-sample-bits", type=int, default=1 << 28)
+    ap.add_argument("--cpu-sample-bits", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain per-op comparison form")
     return ap.parse_args()
+
+
+# ---------------------------------------------------------------- workloads --
+
+class Workload:
+    def __init__(self, name: str, nbits: int, seed: int):
+        from bitstreamzoo_b200 import workloads as wl
+        self.name = name
+        self.nbits = nbits
+        if name == "long_streams":
+            self.src = wl.long_streams_src()
+            self.inputs = wl.long_streams_inputs(nbits, seed=seed)
+            self.out_streams = list(wl.LONG_OUTPUT_STREAMS)
+            self.out_ints = list(wl.LONG_OUTPUT_INTS)
+            self.desc = (f"long_streams: two {nbits}-bit streams; A+B, A<<{{1,63,64,1000}}, A^B, A&~B "
+                         "+ 7 popcounts")
+            self.data = "synthetic (seeded: A ~ Bernoulli(1/2), B all ones with zeros at p=2^-20)"
+        elif name == "regex_dag":
+            self.src = wl.regex_dag_src(2000, seed=20261206)
+            self.inputs = wl.regex_dag_inputs(nbits, seed=seed)
+            self.out_streams = [f"o{j}" for j in range(4)]
+            self.out_ints = [f"p{j}" for j in range(4)]
+            self.desc = (f"regex_dag: seeded 2000-op DAG (55% and/or/xor/andnot, 20% <<1, 10% add, 10% "
+                         f"MatchStar, 5% not; uniform operand choice) over 8 basis streams of {nbits} bits")
+            self.data = ("synthetic (seeded bytes: 70% a-z, 15% 0-9, 10% punctuation, 5% uniform; "
+                         "transposed to basis bits)")
+        else:
+            self.src = wl.MATCHSTAR_SRC
+            self.inputs = wl.matchstar_inputs(nbits, seed=seed)
+            self.out_streams = ["r"]
+            self.out_ints = ["n"]
+            self.desc = f"matchstar: (((M&C)+C)^C)|M + popcount on {nbits}-bit streams"
+            self.data = "synthetic (seeded: M ~ Bernoulli(1/64), C ~ Bernoulli(3/4))"
+        self.stream_bytes = nbits // 8
+        self.in_bytes = len(self.inputs) * self.stream_bytes
+        self.out_bytes = len(self.out_streams) * self.stream_bytes + 8 * len(self.out_ints)
+
+    def kernel_bytes(self, kname: str) -> float:
+        s = self.stream_bytes
+        table = {"k_and": 3 * s, "k_or": 3 * s, "k_xor": 3 * s, "k_andnot": 3 * s, "k_not": 2 * s,
+                 "k_shl": 2 * s, "k_shr": 2 * s, "k_add": 3 * s, "k_popcount": s + 8, "k_fill": s,
+                 "k_any": s}
+        if kname.startswith("fused"):
+            return self.in_bytes + self.out_bytes
+        return table.get(kname, float("nan"))
+
+
+DEFAULT_BITS = {"long_streams": 1 << 32, "regex_dag": 1 << 29, "matchstar": 1 << 24}
+DEFAULT_CPU_SAMPLE = {"long_streams": 1 << 28, "regex_dag": 1 << 26, "matchstar": 1 << 24}
 
 
 def peaks():
@@ -91,6 +145,7 @@ class Clocks:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            time.sleep(0.3)
         except Exception:
             self.proc = None
 
@@ -128,23 +183,22 @@ class Clocks:
 
 # ---------------------------------------------------------------- CPU side --
 
-def cpu_baseline(nbits: int, reps: int, warm: int = 1):
-    """Reference CPU executor (bsim, AVX-512 + OpenMP, all host threads) on a
-    bounded sample of the workload.  Falls back to the C port of the oracle
-    when the reference binary was not built."""
-    from bitstreamzoo_b200 import workloads as wl
+def cpu_baseline(workload: str, nbits: int, reps: int, warm: int = 1):
+    """Reference CPU executor (bsim --backend simd_omp, AVX-512 + OpenMP, all
+    host threads) on a bounded sample of the workload; falls back to the C
+    port of the oracle when the reference binary was not built."""
     from bitstreamzoo_b200.bsdata import write_bsdata
     threads = os.cpu_count() or 1
+    w = Workload(workload, nbits, seed=99)
+    full = DEFAULT_BITS[workload]
     bsim = os.path.join(ROOT, "oracle", "_ref", "bsim")
-    inputs = wl.long_streams_inputs(nbits, seed=99)
-    in_bytes = 2 * nbits // 8
     if os.path.exists(bsim):
         with tempfile.TemporaryDirectory() as td:
-            prog = os.path.join(td, "long_streams.bs")
+            prog = os.path.join(td, f"{workload}.bs")
             with open(prog, "w") as f:
-                f.write(wl.long_streams_src())
+                f.write(w.src)
             data = os.path.join(td, "in.bsdata")
-            write_bsdata(data, nbits, inputs)
+            write_bsdata(data, nbits, w.inputs)
             env = dict(os.environ, OMP_NUM_THREADS=str(threads),
                        GLIBC_TUNABLES="glibc.cpu.x86_rep_stosb_threshold=2000000000")
             times = []
@@ -153,7 +207,7 @@ def cpu_baseline(nbits: int, reps: int, warm: int = 1):
                 with open(out, "w") as fo:
                     r = subprocess.run([bsim, prog, "--backend", "simd_omp", "--reuse-mem",
                                         "--input", data], stdout=fo, stderr=subprocess.PIPE,
-                                       env=env, timeout=600)
+                                       env=env, timeout=900)
                 if r.returncode != 0:
                     raise RuntimeError(r.stderr.decode()[-500:])
                 with open(out, "rb") as fi:
@@ -162,38 +216,41 @@ def cpu_baseline(nbits: int, reps: int, warm: int = 1):
                 if i >= warm:
                     times.append(ms)
         ms = statistics.median(times)
-        return {"value": in_bytes / (ms * 1e-3) / 1e9, "unit": "GB/s", "cores": threads,
+        return {"value": w.in_bytes / (ms * 1e-3) / 1e9, "unit": "GB/s", "cores": threads,
                 "kind": "reference", "ms_per_step": ms,
-                "sample": (f"long_streams program at {nbits} bits (1/{(1 << 32) // nbits} of the "
-                           f"2^32-bit workload), bsim --backend simd_omp, OMP_NUM_THREADS={threads}, "
-                           f"median exec_ms of {len(times)} runs")}
-    # C port of the oracle
+                "sample": (f"{workload} program at {nbits} bits per stream (1/{max(1, full // nbits)} "
+                           f"of the {full}-bit workload), bsim --backend simd_omp, "
+                           f"OMP_NUM_THREADS={threads}, median exec_ms of {len(times)} runs")}
     from oracle import cwords, pyoracle
-    prog = pyoracle.parse(wl.long_streams_src())
+    prog = pyoracle.parse(w.src)
     times = []
     for i in range(warm + reps):
         t0 = time.perf_counter()
-        cwords.run_straight_line(prog, nbits, inputs)
+        cwords.run_straight_line(prog, nbits, w.inputs)
         if i >= warm:
             times.append((time.perf_counter() - t0) * 1e3)
     ms = statistics.median(times)
-    return {"value": in_bytes / (ms * 1e-3) / 1e9, "unit": "GB/s",
+    return {"value": w.in_bytes / (ms * 1e-3) / 1e9, "unit": "GB/s",
             "cores": cwords.lib().o_num_threads(), "kind": "port", "ms_per_step": ms,
-            "sample": f"long_streams program at {nbits} bits, oracle C port, median of {len(times)}"}
+            "sample": f"{workload} at {nbits} bits per stream, oracle C port, median of {len(times)}"}
+
+
+def metric_name(workload: str) -> str:
+    return f"input GB/s ({workload}, bit-exact)"
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
     steps = max(1, min(args.steps, 5))
-    cb = cpu_baseline(args.cpu_sample_bits, steps, warm=min(1, args.warmup))
-    line = {"metric": "input GB/s (long-stream primitives, bit-exact)", "value": cb["value"],
-            "unit": "GB/s", "n_gpus": 0, "steps": steps, "warmup": min(1, args.warmup),
-            "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": f"{WORKLOAD}: A+B, A<<{{1,63,64,1000}}, A^B, A&~B, popcounts; "
-                                   f"sample {args.cpu_sample_bits} bits of 2^32"},
+    warm = min(1, args.warmup)
+    sample = args.cpu_sample_bits or DEFAULT_CPU_SAMPLE[args.workload]
+    cb = cpu_baseline(args.workload, sample, steps, warm=warm)
+    line = {"metric": metric_name(args.workload), "value": cb["value"], "unit": "GB/s",
+            "n_gpus": 0, "steps": steps, "warmup": warm, "ms_per_step": cb["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"{args.workload}; CPU sample of {sample} bits per stream"},
             "cpu_baseline": {k: cb[k] for k in ("kind", "cores", "sample", "value", "unit")},
             "e2e": {"value": cb["value"], "unit": "GB/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -201,17 +258,6 @@ def run_reference(args, rank, world):
 
 
 # ---------------------------------------------------------------- GPU side --
-
-# Algorithmic bytes per launch for each kernel, as a function of N (bits).
-def kernel_bytes(name: str, nbits: int, n_out_streams: int = 7, n_pops: int = 7) -> float:
-    s = nbits / 8
-    table = {"k_and": 3 * s, "k_or": 3 * s, "k_xor": 3 * s, "k_andnot": 3 * s, "k_not": 2 * s,
-             "k_shl": 2 * s, "k_shr": 2 * s, "k_add": 3 * s, "k_popcount": s + 8, "k_fill": s,
-             "k_any": s}
-    if name.startswith("fused"):
-        return 2 * s + n_out_streams * s + 8 * n_pops
-    return table.get(name, float("nan"))
-
 
 def run_ours(args, rank, world, local):
     import torch
@@ -226,16 +272,14 @@ def run_ours(args, rank, world, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     hbm, hbm_src = peaks()
-    nbits = args.nbits
+    nbits = args.nbits or DEFAULT_BITS[args.workload]
     nw = wl.n_words(nbits)
+    W = Workload(args.workload, nbits, seed=20261204 + rank)
     ctx = bz.Context(local)
     ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
-    prog = ctx.compile(wl.long_streams_src())
-    host = wl.long_streams_inputs(nbits, seed=20261204 + rank)
-    dA = torch.from_numpy(host["A"].view(np.int64)).to(dev)
-    dB = torch.from_numpy(host["B"].view(np.int64)).to(dev)
+    prog = ctx.compile(W.src)
+    dev_in = {k: torch.from_numpy(v.view(np.int64)).to(dev) for k, v in W.inputs.items()}
     torch.cuda.synchronize()
-    in_bytes = 2 * nbits // 8
     mode_of = {"fused": bz.MODE_FUSED, "plain": bz.MODE_PLAIN}
 
     def barrier():
@@ -252,15 +296,15 @@ def run_ours(args, rank, world, local):
 
     def step(mode):
         r = prog.run(nbits, mode)
-        r.bind("A", ("borrow", dA.data_ptr(), nw))
-        r.bind("B", ("borrow", dB.data_ptr(), nw))
+        for k, t in dev_in.items():
+            r.bind(k, ("borrow", t.data_ptr(), nw))
         st = r.execute()
-        pops = {n: r.int(n) for n in wl.LONG_OUTPUT_INTS}
+        pops = {n: r.int(n) for n in W.out_ints}
         del r
         return st, pops
 
     forms = {}
-    order = [args.mode] + [m for m in ("fused", "plain") if m != args.mode]
+    order = [args.mode] + ([] if args.no_plain else [m for m in ("fused", "plain") if m != args.mode])
     for name in order:
         mode = mode_of[name]
         try:
@@ -269,6 +313,7 @@ def run_ours(args, rank, world, local):
         except bz.BszError as e:
             forms[name] = {"unavailable": str(e)[:200]}
             continue
+        compile_ms = st.get("compile_ms", 0.0)
         barrier()
         ctx.profile(True)
         clocks = Clocks(local)
@@ -276,10 +321,11 @@ def run_ours(args, rank, world, local):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(ext)
-        launches = 0
+        launches = fallbacks = 0
         for _ in range(args.steps):
             st, pops = step(mode)
             launches += st["n_kernel_launches"]
+            fallbacks += st["n_fused_fallbacks"]
         e1.record(ext)
         e1.synchronize()
         barrier()
@@ -288,38 +334,42 @@ def run_ours(args, rank, world, local):
         prof = ctx.profile_report()
         ctx.profile(False)
         ms_max = max_over_ranks(ms)
-        forms[name] = {"ms": ms_max, "launches": launches, "profile": prof, "clocks": ck,
-                       "pops": pops,
-                       "value": world * in_bytes * args.steps / (ms_max * 1e-3) / 1e9}
+        forms[name] = {"ms": ms_max, "launches": launches, "fused_fallbacks": fallbacks,
+                       "profile": prof, "clocks": ck, "pops": pops,
+                       "value": world * W.in_bytes * args.steps / (ms_max * 1e-3) / 1e9,
+                       "hbm_frac_step": ((W.in_bytes + W.out_bytes) * args.steps / (ms_max * 1e-3) / 1e9) / hbm}
 
-    # sanity (bit-exact popcounts that are cheap to check on the host)
-    ref_px = int(np.bitwise_count(host["A"] ^ host["B"]).sum())
-    ref_pl64 = int(np.bitwise_count(host["A"][:-1]).sum())
-    for name, f in forms.items():
-        if "pops" in f:
-            f["check"] = (f["pops"]["px"] == ref_px and f["pops"]["pl64"] == ref_pl64)
+    # cheap host checks of popcounts the two forms must agree on (and, for the
+    # long-stream workload, two that numpy computes exactly)
+    if "pops" in forms.get("fused", {}) and "pops" in forms.get("plain", {}):
+        forms["fused"]["agrees_with_plain"] = forms["fused"]["pops"] == forms["plain"]["pops"]
+    if args.workload == "long_streams":
+        ref_px = int(np.bitwise_count(W.inputs["A"] ^ W.inputs["B"]).sum())
+        ref_pl64 = int(np.bitwise_count(W.inputs["A"][:-1]).sum())
+        for f in forms.values():
+            if "pops" in f:
+                f["check"] = (f["pops"]["px"] == ref_px and f["pops"]["pl64"] == ref_pl64)
 
-    # end to end through the C ABI: pinned host in, all outputs out
+    # end to end through the C ABI: pinned host in, every output out
     e2e = None
     main = forms.get(args.mode, {})
     if not args.no_e2e and "ms" in main:
         mode = mode_of[args.mode]
-        pA = torch.from_numpy(host["A"].view(np.int64)).pin_memory()
-        pB = torch.from_numpy(host["B"].view(np.int64)).pin_memory()
-        outs = {n: torch.empty(nw, dtype=torch.int64).pin_memory() for n in wl.LONG_OUTPUT_STREAMS}
-        a_np, b_np = pA.numpy().view(np.uint64), pB.numpy().view(np.uint64)
-        o_np = {n: t.numpy().view(np.uint64) for n, t in outs.items()}
+        pinned_in = {k: torch.from_numpy(v.view(np.int64)).pin_memory() for k, v in W.inputs.items()}
+        pinned_out = {n: torch.empty(nw, dtype=torch.int64).pin_memory() for n in W.out_streams}
+        in_np = {k: t.numpy().view(np.uint64) for k, t in pinned_in.items()}
+        out_np = {n: t.numpy().view(np.uint64) for n, t in pinned_out.items()}
 
         def e2e_step():
             r = prog.run(nbits, mode)
-            r.bind("A", a_np)
-            r.bind("B", b_np)
+            for k, a in in_np.items():
+                r.bind(k, a)
             r.execute()
-            for n in wl.LONG_OUTPUT_STREAMS:
-                bz._lib.check(r.lib.bsz_get_stream(r.h, n.encode(), -1, o_np[n].ctypes.data, nw))
-            pops = [r.int(n) for n in wl.LONG_OUTPUT_INTS]
+            for n in W.out_streams:
+                bz._lib.check(r.lib.bsz_get_stream(r.h, n.encode(), -1, out_np[n].ctypes.data, nw))
+            vals = [r.int(n) for n in W.out_ints]
             del r
-            return pops
+            return vals
 
         for _ in range(max(1, min(args.warmup, 2))):
             e2e_step()
@@ -336,59 +386,52 @@ def run_ours(args, rank, world, local):
         wall = (time.perf_counter() - t0) * 1e3
         barrier()
         ms = max_over_ranks(max(e0.elapsed_time(e1), wall))
-        e2e = {"value": world * in_bytes * k / (ms * 1e-3) / 1e9, "unit": "GB/s",
-               "h2d_bytes_per_step": in_bytes,
-               "d2h_bytes_per_step": len(wl.LONG_OUTPUT_STREAMS) * nw * 8 + 8 * len(wl.LONG_OUTPUT_INTS),
+        e2e = {"value": world * W.in_bytes * k / (ms * 1e-3) / 1e9, "unit": "GB/s",
+               "h2d_bytes_per_step": W.in_bytes, "d2h_bytes_per_step": len(W.out_streams) * nw * 8 + 8 * len(W.out_ints),
                "steps": k, "ms_per_step": ms / k}
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cb = cpu_baseline(args.cpu_sample_bits, 3)
+            cb = cpu_baseline(args.workload, args.cpu_sample_bits or DEFAULT_CPU_SAMPLE[args.workload], 3)
         except Exception as e:  # noqa: BLE001
             cb = {"unavailable": str(e)[:200]}
 
     if rank == 0:
-        main = forms.get(args.mode, {})
-        value = main.get("value")
         prof = main.get("profile", {})
         roof = None
         if prof:
-            top = max(prof.items(), key=lambda kv: kv[1]["ms"])
-            kname, kv = top
+            kname, kv = max(prof.items(), key=lambda kv: kv[1]["ms"])
             per_launch_ms = kv["ms"] / max(1, kv["launches"])
-            bytes_launch = kernel_bytes(kname, nbits)
+            bytes_launch = W.kernel_bytes(kname)
             achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
             traffic = None
             tpath = os.path.join(ROOT, "profiles", "traffic.json")
             if os.path.exists(tpath):
                 with open(tpath) as f:
-                    traffic = json.load(f).get(kname)
+                    traffic = json.load(f).get(f"{args.workload}:{kname}")
             roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
                     "peak_source": hbm_src, "unit": "GB/s", "frac": achieved / hbm,
                     "traffic": traffic, "bytes_per_launch": bytes_launch,
                     "launch_ms": per_launch_ms,
                     "kernel_share": kv["ms"] / max(1e-9, sum(x["ms"] for x in prof.values()))}
-        step_bytes = in_bytes + 7 * nbits // 8 + 56
         line = {
-            "metric": "input GB/s (long-stream primitives, bit-exact)",
-            "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "metric": metric_name(args.workload),
+            "value": main.get("value"), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": main.get("ms", float("nan")) / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
-            "data": "synthetic (seeded: A ~ Bernoulli(1/2), B ones with zeros at p=2^-20)",
-            "config": {"workload": (f"{WORKLOAD}: two {nbits}-bit streams per GPU; A+B, "
-                                    "A<<{1,63,64,1000}, A^B, A&~B + 7 popcounts"),
-                       "form": args.mode, "bits_per_stream": nbits,
-                       "l2": "inputs (1 GiB/GPU) larger than L2; no flush needed",
-                       "parallelism": f"replicas x{world} (independent stream pairs)"},
-            "hbm_frac_step": (step_bytes * args.steps / (main.get("ms", float("nan")) * 1e-3) / 1e9) / hbm
-            if main.get("ms") else None,
+            "data": W.data,
+            "config": {"workload": W.desc + " (per GPU)", "form": args.mode, "bits_per_stream": nbits,
+                       "l2": ("inputs larger than L2; no flush needed" if W.in_bytes > (126 << 20)
+                              else "inputs fit in L2 (reported, not roofline-judged)"),
+                       "parallelism": f"replicas x{world} (independent stream sets)"},
+            "hbm_frac_step": main.get("hbm_frac_step"),
             "roofline": roof,
             "cpu_baseline": cb,
             "e2e": e2e,
             "gpu_launches": main.get("launches"),
             "clocks": main.get("clocks"),
-            "forms": {k: {kk: vv for kk, vv in v.items() if kk not in ("pops",)} for k, v in forms.items()},
+            "forms": {k: {kk: vv for kk, vv in v.items() if kk != "pops"} for k, v in forms.items()},
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -28,6 +28,9 @@ from ._lib import BszError, Stats
 MODE_PLAIN = 0
 MODE_FUSED = 1
 
+DEFAULT_SCHEDULE = {"warps": 4, "range_steps": 64, "ctas_per_sm": 0, "min_blocks": 4,
+                    "prefetch": 1, "cut_adds": 0}
+
 __all__ = ["Context", "Program", "Run", "B200Backend", "BszError", "MODE_PLAIN", "MODE_FUSED",
            "int_to_words", "words_to_int", "bsim_cuda_path"]
 
@@ -132,6 +135,12 @@ class Context:
         _lib.check(self.lib.bsz_op_popcount(self.h, a_ptr, nw, ctypes.byref(out)))
         return out.value
 
+    def s2p(self, bytes_ptr: int, n_bytes: int, basis_ptrs) -> None:
+        """Device byte -> basis-bit transposition into eight device streams of
+        ``ceil(n_bytes / 64)`` words (asynchronous on the context's stream)."""
+        arr = (ctypes.c_void_p * 8)(*[int(p) for p in basis_ptrs])
+        _lib.check(self.lib.bsz_s2p(self.h, bytes_ptr, int(n_bytes), arr))
+
     def is_nonzero(self, a_ptr: int, nw: int) -> bool:
         out = ctypes.c_int()
         _lib.check(self.lib.bsz_op_is_nonzero(self.h, a_ptr, nw, ctypes.byref(out)))
@@ -186,6 +195,13 @@ class Run:
 
     def set_param(self, name: str, value: int):
         _lib.check(self.lib.bsz_set_param(self.h, name.encode(), int(value)))
+
+    def set_schedule(self, schedule: dict):
+        """Fused-kernel schedule: keys of ``DEFAULT_SCHEDULE`` (missing keys keep defaults)."""
+        s = dict(DEFAULT_SCHEDULE)
+        s.update(schedule or {})
+        st = _lib.Schedule(**{k: int(s[k]) for k, _ in _lib.Schedule._fields_})
+        _lib.check(self.lib.bsz_run_set_schedule(self.h, ctypes.byref(st)))
 
     def bind(self, name: str, value, index: int = -1, tail: int = 0):
         """Bind a Python int, a numpy uint64 array, or a device pointer:
@@ -243,6 +259,63 @@ class Run:
     def has_stream(self, name: str) -> bool:
         out = np.empty(1, dtype=np.uint64)
         return self.lib.bsz_get_stream(self.h, name.encode(), -1, out.ctypes.data, 0) == 0
+
+
+class Batch:
+    """Many instances of several straight-line programs in one graph-captured launch.
+
+    ``instances`` is a list of ``(program_index, bitlength, input_ptrs, output_ptrs)``
+    with device pointers (ints) in the order of each program's declared scalar
+    inputs / output streams (0 = do not store that output).
+    """
+
+    def __init__(self, ctx: Context, programs: list, instances: list, schedule: dict | None = None):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.programs = programs
+        n = len(instances)
+        self._keep = []
+        arr = (_lib.Instance * max(1, n))()
+        for i, (p, bits, ins, outs) in enumerate(instances):
+            ia = (ctypes.c_void_p * max(1, len(ins)))(*ins)
+            oa = (ctypes.c_void_p * max(1, len(outs)))(*[o or None for o in outs])
+            self._keep += [ia, oa]
+            arr[i].program = p
+            arr[i].bitlength = bits
+            arr[i].inputs = ctypes.cast(ia, ctypes.POINTER(ctypes.c_void_p))
+            arr[i].outputs = ctypes.cast(oa, ctypes.POINTER(ctypes.c_void_p))
+        s = dict(DEFAULT_SCHEDULE)
+        s.update(schedule or {})
+        st = _lib.Schedule(**{k: int(s[k]) for k, _ in _lib.Schedule._fields_})
+        progs = (ctypes.c_void_p * len(programs))(*[p.h for p in programs])
+        self.n = n
+        self.h = self.lib.bsz_batch_create(ctx.h, progs, len(programs), arr, n, ctypes.byref(st))
+        if not self.h:
+            raise BszError(_lib.last_error())
+        self.items = self.lib.bsz_batch_items(self.h)
+
+    def launch(self):
+        _lib.check(self.lib.bsz_batch_launch(self.h))
+
+    def finish(self) -> dict:
+        st = Stats()
+        _lib.check(self.lib.bsz_batch_finish(self.h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def ints(self, instance: int) -> list[int]:
+        buf = (ctypes.c_int64 * 64)()
+        n = self.lib.bsz_batch_ints(self.h, instance, buf, 64)
+        if n < 0:
+            raise BszError(_lib.last_error())
+        return list(buf[:n])
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.lib.bsz_batch_free(self.h)
+                self.h = None
+        except Exception:
+            pass
 
 
 def _source_of(prog) -> str:

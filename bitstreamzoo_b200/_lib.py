@@ -29,6 +29,20 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Schedule(ctypes.Structure):
+    _fields_ = [("warps", ctypes.c_int32), ("range_steps", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32), ("min_blocks", ctypes.c_int32),
+                ("prefetch", ctypes.c_int32), ("cut_adds", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Instance(ctypes.Structure):
+    _fields_ = [("program", ctypes.c_int32), ("bitlength", ctypes.c_int64),
+                ("inputs", ctypes.POINTER(ctypes.c_void_p)), ("outputs", ctypes.POINTER(ctypes.c_void_p))]
+
+
 # name -> (restype, argtypes); every symbol declared in include/bsz.h
 SIGNATURES = {
     "bsz_version": (ctypes.c_char_p, []),
@@ -45,6 +59,7 @@ SIGNATURES = {
     "bsz_run_create": (c_void_p, [c_void_p, ctypes.c_int64, ctypes.c_int]),
     "bsz_run_free": (None, [c_void_p]),
     "bsz_set_param": (ctypes.c_int, [c_void_p, ctypes.c_char_p, ctypes.c_int64]),
+    "bsz_run_set_schedule": (ctypes.c_int, [c_void_p, ctypes.POINTER(Schedule)]),
     "bsz_bind_input": (ctypes.c_int, [c_void_p, ctypes.c_char_p, ctypes.c_int64, c_void_p,
                                       ctypes.c_uint64, ctypes.c_int, ctypes.c_int]),
     "bsz_bind_broadcast": (ctypes.c_int, [c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint8),
@@ -56,6 +71,23 @@ SIGNATURES = {
                                              ctypes.POINTER(c_void_p)]),
     "bsz_get_int": (ctypes.c_int, [c_void_p, ctypes.c_char_p, i64p]),
     "bsz_array_indices": (ctypes.c_int64, [c_void_p, ctypes.c_char_p, i64p, ctypes.c_int64]),
+    "bsz_batch_create": (c_void_p, [c_void_p, ctypes.POINTER(c_void_p), ctypes.c_int,
+                                    ctypes.POINTER(Instance), ctypes.c_int64, ctypes.POINTER(Schedule)]),
+    "bsz_batch_launch": (ctypes.c_int, [c_void_p]),
+    "bsz_batch_finish": (ctypes.c_int, [c_void_p, ctypes.POINTER(Stats)]),
+    "bsz_batch_ints": (ctypes.c_int, [c_void_p, ctypes.c_int64, i64p, ctypes.c_int]),
+    "bsz_batch_items": (ctypes.c_int64, [c_void_p]),
+    "bsz_batch_free": (None, [c_void_p]),
+    "bsz_program_features": (ctypes.c_int, [c_void_p, c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
+    "bsz_mlp_create": (c_void_p, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64]),
+    "bsz_mlp_num_params": (ctypes.c_int64, [c_void_p]),
+    "bsz_mlp_train_step": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int, ctypes.c_float,
+                                          ctypes.POINTER(ctypes.c_float)]),
+    "bsz_mlp_predict": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_void_p]),
+    "bsz_mlp_gradients": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int, c_void_p,
+                                         ctypes.POINTER(ctypes.c_float)]),
+    "bsz_mlp_params": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int]),
+    "bsz_mlp_free": (None, [c_void_p]),
     "bsz_run_case_json": (ctypes.c_char_p, [c_void_p, ctypes.c_char_p, ctypes.c_char_p,
                                             ctypes.c_char_p, ctypes.c_int]),
     "bsz_op_not": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_uint64, ctypes.c_int64]),
@@ -72,6 +104,7 @@ SIGNATURES = {
     "bsz_op_popcount": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_uint64, u64p]),
     "bsz_add_noalloc": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_uint64, ctypes.c_int64,
                                        c_void_p]),
+    "bsz_s2p": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, ctypes.POINTER(c_void_p)]),
     "bsz_op_is_nonzero": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_uint64,
                                          ctypes.POINTER(ctypes.c_int)]),
 }

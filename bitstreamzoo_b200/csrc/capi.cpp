@@ -11,7 +11,9 @@
 #include "device.h"
 #include "engine.h"
 #include "frontend.h"
+#include "fused.h"
 #include "io.h"
+#include "mlp.h"
 
 // Lifetimes: runs keep their program alive and programs keep their context
 // alive, so the handles may be freed in any order.
@@ -194,6 +196,19 @@ int bsz_set_param(bsz_run* run, const char* name, int64_t value) {
   });
 }
 
+int bsz_run_set_schedule(bsz_run* run, const bsz_schedule* s) {
+  return guard([&] {
+    bsz::Schedule c;
+    c.warps = s->warps;
+    c.range_steps = s->range_steps;
+    c.ctas_per_sm = s->ctas_per_sm;
+    c.min_blocks = s->min_blocks;
+    c.prefetch = s->prefetch;
+    c.cut_adds = s->cut_adds;
+    executor(run).set_schedule(c);
+  });
+}
+
 int bsz_bind_input(bsz_run* run, const char* name, int64_t index, const uint64_t* words,
                    uint64_t n_words, int tail, int on_device) {
   return guard([&] {
@@ -322,6 +337,226 @@ int64_t bsz_array_indices(bsz_run* run, const char* name, int64_t* indices, int6
   return count;
 }
 
+int bsz_program_features(bsz_ctx* ctx, bsz_program* prog, float* out, int capacity) {
+  int count = -1;
+  guard([&] {
+    bsz::ExecOptions eo;
+    eo.mode = bsz::ExecMode::Fused;
+    bsz::Executor ex(*ctx->dev, *prog->prog, int64_t(1) << 20, eo);
+    bsz::Executor::Traced t = ex.trace();
+    const auto& nd = t.nodes;
+    std::vector<uint8_t> live(nd.size(), 0);
+    std::vector<int> stack;
+    for (int n : t.output_nodes)
+      if (n >= 0) stack.push_back(n);
+    for (auto& p : t.pops) stack.push_back(p.first);
+    while (!stack.empty()) {
+      int n = stack.back();
+      stack.pop_back();
+      if (live[n]) continue;
+      live[n] = 1;
+      for (int o : {nd[n].a, nd[n].b})
+        if (o >= 0) stack.push_back(o);
+    }
+    auto is_leaf = [&](int n) {
+      auto op = nd[n].op;
+      return op == bsz::NOp::Buf || op == bsz::NOp::Zero || op == bsz::NOp::OnesMask ||
+             op == bsz::NOp::AllOnes;
+    };
+    double n_ops = 0, n_bit = 0, n_not = 0, n_shl_t = 0, n_shl_i = 0, n_add = 0, n_shr = 0, n_in = 0;
+    double max_ws = 0;
+    std::vector<int> depth(nd.size(), 0), adepth(nd.size(), 0);
+    int max_depth = 0, max_adepth = 0;
+    for (size_t i = 0; i < nd.size(); ++i) {
+      if (!live[i]) continue;
+      const bsz::Node& x = nd[i];
+      if (is_leaf(static_cast<int>(i))) {
+        if (x.op == bsz::NOp::Buf) ++n_in;
+        continue;
+      }
+      ++n_ops;
+      int d = 0, ad = 0;
+      for (int o : {x.a, x.b})
+        if (o >= 0) {
+          d = std::max(d, depth[o]);
+          ad = std::max(ad, adepth[o]);
+        }
+      depth[i] = d + 1;
+      adepth[i] = ad + (x.op == bsz::NOp::Add ? 1 : 0);
+      max_depth = std::max(max_depth, depth[i]);
+      max_adepth = std::max(max_adepth, adepth[i]);
+      switch (x.op) {
+        case bsz::NOp::And: case bsz::NOp::Or: case bsz::NOp::Xor: ++n_bit; break;
+        case bsz::NOp::Not: case bsz::NOp::AndNot: ++n_not; break;
+        case bsz::NOp::Add: ++n_add; break;
+        case bsz::NOp::Shr: ++n_shr; max_ws = std::max<double>(max_ws, x.k / 64.0); break;
+        case bsz::NOp::Shl:
+          if (is_leaf(x.a)) ++n_shl_i;
+          else ++n_shl_t;
+          max_ws = std::max<double>(max_ws, x.k / 64.0);
+          break;
+        default: break;
+      }
+    }
+    const double tot = std::max(1.0, n_ops);
+    const float f[BSZ_NUM_FEATURES] = {
+        static_cast<float>(std::log2(1 + n_ops)), static_cast<float>(n_bit / tot),
+        static_cast<float>(n_not / tot), static_cast<float>(n_shl_t / tot),
+        static_cast<float>(n_shl_i / tot), static_cast<float>(n_add / tot),
+        static_cast<float>(n_shr / tot), static_cast<float>(std::log2(1.0 + max_depth)),
+        static_cast<float>(std::log2(1.0 + max_adepth)), static_cast<float>(std::log2(1 + max_ws)),
+        static_cast<float>(std::log2(1 + n_in)),
+        static_cast<float>(std::log2(1.0 + t.output_nodes.size() + t.pops.size())),
+        static_cast<float>(std::log2(1 + n_shl_t)), static_cast<float>(std::log2(1 + n_add))};
+    for (int i = 0; i < BSZ_NUM_FEATURES && i < capacity; ++i) out[i] = f[i];
+    count = BSZ_NUM_FEATURES;
+  });
+  return count;
+}
+
+struct bsz_mlp {
+  bsz_ctx* ctx;
+  std::unique_ptr<bsz::Mlp> net;
+};
+
+bsz_mlp* bsz_mlp_create(bsz_ctx* ctx, int in_dim, int hidden, int layers, uint64_t seed) {
+  bsz_mlp* out = nullptr;
+  if (guard([&] {
+        auto m = std::make_unique<bsz_mlp>();
+        m->ctx = ctx;
+        m->net = std::make_unique<bsz::Mlp>(in_dim, hidden, layers, seed, ctx->dev->stream());
+        ++ctx->refs;
+        out = m.release();
+      }))
+    return nullptr;
+  return out;
+}
+
+int64_t bsz_mlp_num_params(bsz_mlp* m) { return m->net->n_params(); }
+
+int bsz_mlp_train_step(bsz_mlp* m, const float* x, const float* y, int n, float lr, float* loss) {
+  return guard([&] {
+    float l = m->net->train_step(x, y, n, lr);
+    if (loss) *loss = l;
+  });
+}
+
+int bsz_mlp_predict(bsz_mlp* m, const float* x, int n, float* out) {
+  return guard([&] { m->net->predict(x, n, out); });
+}
+
+int bsz_mlp_gradients(bsz_mlp* m, const float* x, const float* y, int n, float* grad, float* loss) {
+  return guard([&] {
+    float l = m->net->gradients(x, y, n, grad);
+    if (loss) *loss = l;
+  });
+}
+
+int bsz_mlp_params(bsz_mlp* m, float* params, int get) {
+  return guard([&] {
+    if (get) m->net->get_params(params);
+    else m->net->set_params(params);
+  });
+}
+
+void bsz_mlp_free(bsz_mlp* m) {
+  if (!m) return;
+  bsz_ctx* c = m->ctx;
+  m->net.reset();
+  delete m;
+  ctx_unref(c);
+}
+
+struct bsz_batch {
+  bsz_ctx* ctx;
+  std::vector<bsz_program*> progs;
+  std::unique_ptr<bsz::BatchRunner> runner;
+  int64_t launches0 = 0;
+};
+
+bsz_batch* bsz_batch_create(bsz_ctx* ctx, bsz_program* const* programs, int n_programs,
+                            const bsz_instance* instances, int64_t n_instances,
+                            const bsz_schedule* schedule) {
+  bsz_batch* out = nullptr;
+  if (guard([&] {
+        auto b = std::make_unique<bsz_batch>();
+        b->ctx = ctx;
+        std::vector<const bsz::Program*> progs;
+        for (int i = 0; i < n_programs; ++i) {
+          b->progs.push_back(programs[i]);
+          progs.push_back(programs[i]->prog.get());
+        }
+        std::vector<bsz::BatchInstance> inst(static_cast<size_t>(n_instances));
+        for (int64_t i = 0; i < n_instances; ++i) {
+          const bsz_instance& x = instances[i];
+          if (x.program < 0 || x.program >= n_programs)
+            throw std::invalid_argument("bsz_batch_create: program index out of range");
+          const bsz::Program& p = *progs[x.program];
+          inst[i].program = x.program;
+          inst[i].bitlength = x.bitlength;
+          inst[i].inputs.assign(x.inputs, x.inputs + p.inputs.size());
+          inst[i].outputs.assign(x.outputs, x.outputs + p.outputs.size());
+        }
+        bsz::Schedule s;
+        if (schedule) {
+          s.warps = std::max(1, std::min(schedule->warps, 16));
+          s.range_steps = std::max(1, schedule->range_steps);
+          s.ctas_per_sm = std::max(0, schedule->ctas_per_sm);
+          s.min_blocks = std::max(1, schedule->min_blocks);
+          s.prefetch = schedule->prefetch;
+          s.cut_adds = 0;
+        }
+        b->runner = std::make_unique<bsz::BatchRunner>(*ctx->dev, progs, std::move(inst), s);
+        for (auto* p : b->progs) ++p->refs;
+        out = b.release();
+      }))
+    return nullptr;
+  return out;
+}
+
+int bsz_batch_launch(bsz_batch* b) {
+  return guard([&] {
+    b->launches0 = b->ctx->dev->n_launches;
+    b->runner->launch();
+  });
+}
+
+int bsz_batch_finish(bsz_batch* b, bsz_stats* stats) {
+  return guard([&] {
+    b->runner->finish();
+    if (uint32_t e = b->ctx->dev->take_error())
+      throw bsz::RuntimeError("device error word " + std::to_string(e));
+    if (stats) {
+      std::memset(stats, 0, sizeof(*stats));
+      stats->n_kernel_launches = b->ctx->dev->n_launches - b->launches0;
+      stats->n_mallocs = b->ctx->dev->n_mallocs;
+      stats->n_fused_launches = b->runner->launches;
+      stats->n_fused_fallbacks = b->runner->fallbacks;
+      stats->compile_ms = b->runner->compile_ms;
+      stats->n_segments = 1;
+    }
+  });
+}
+
+int bsz_batch_ints(bsz_batch* b, int64_t instance, int64_t* values, int capacity) {
+  int n = -1;
+  guard([&] {
+    const auto& v = b->runner->ints(instance);
+    n = static_cast<int>(v.size());
+    for (int i = 0; i < n && i < capacity; ++i) values[i] = v[i];
+  });
+  return n;
+}
+
+int64_t bsz_batch_items(bsz_batch* b) { return b->runner->n_items(); }
+
+void bsz_batch_free(bsz_batch* b) {
+  if (!b) return;
+  b->runner.reset();
+  for (auto* p : b->progs) prog_unref(p);
+  delete b;
+}
+
 const char* bsz_run_case_json(bsz_ctx* ctx, const char* source, const char* bsdata_path,
                               const char* json_input, int flags) {
   g_json.clear();
@@ -396,6 +631,14 @@ int bsz_op_popcount(bsz_ctx* ctx, const uint64_t* a, uint64_t n, uint64_t* resul
     dev.sync();
   });
 }
+int bsz_s2p(bsz_ctx* ctx, const uint8_t* bytes, int64_t n_bytes, uint64_t* const* basis) {
+  return guard([&] {
+    if (n_bytes < 0) throw bsz::RuntimeError("bsz_s2p: negative byte count");
+    if (n_bytes > 0 && (!bytes || !basis)) throw bsz::RuntimeError("bsz_s2p: null pointer");
+    bsz::launch_s2p(*ctx->dev, bytes, n_bytes, basis);
+  });
+}
+
 int bsz_op_is_nonzero(bsz_ctx* ctx, const uint64_t* a, uint64_t n, int* result) {
   return guard([&] {
     bsz::Device& dev = *ctx->dev;

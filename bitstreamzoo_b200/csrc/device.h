@@ -149,6 +149,9 @@ void launch_popcount(Device& dev, const uint64_t* a, int64_t n,
 void launch_any(Device& dev, const uint64_t* a, int64_t n, unsigned int* flag);
 void launch_fill(Device& dev, uint64_t* d, int64_t n, uint64_t value, uint64_t last_value);
 void launch_copy(Device& dev, uint64_t* d, const uint64_t* a, int64_t n);
+// Byte -> basis bits (s2p.cu): out[i] (ceil(n_bytes/64) words each) gets bit i
+// of every byte.
+void launch_s2p(Device& dev, const uint8_t* bytes, int64_t n_bytes, uint64_t* const* out);
 
 inline uint64_t mask_for_bits(int64_t nbits) {
   int r = static_cast<int>(nbits & 63);

@@ -58,6 +58,11 @@ Executor::~Executor() {
   if (d_slots_) cudaFree(d_slots_);
 }
 
+void Executor::set_schedule(const Schedule& s) {
+  opt_.sched = s;
+  if (fused_) fused_->set_schedule(s);
+}
+
 int64_t Executor::fused_launches() const { return fused_ ? fused_->launches : 0; }
 int64_t Executor::fused_fallbacks() const { return fused_ ? fused_->fallbacks : 0; }
 
@@ -170,7 +175,7 @@ int Executor::mk(NOp op, int a, int b, int64_t k) {
         if (is(b, NOp::Zero) && clean(a)) return a;
         break;
       case NOp::Shl:
-        if (is(a, NOp::Zero) || k >= N_) return zero_;
+        if (is(a, NOp::Zero) || (!tracing_ && k >= N_)) return zero_;
         if (k == 0 && clean(a)) return a;
         break;
       case NOp::Shr:
@@ -296,8 +301,8 @@ Executor::IntV Executor::popcount(int node) {
   if (n.tail) throw RuntimeError("popcount on negative value (infinite bits set)");
   count("popcount");
   if (n.op == NOp::Zero) return IntV{0, -1};
-  if (n.op == NOp::OnesMask) return IntV{N_, -1};
-  ensure_slots(1);
+  if (n.op == NOp::OnesMask && !tracing_) return IntV{N_, -1};
+  if (!tracing_) ensure_slots(1);
   int64_t slot = n_slots_++;
   pending_pops_.push_back({node, slot});
   iexpr_.push_back(IE{'s', -1, -1, slot});
@@ -424,6 +429,10 @@ void Executor::run() {
 // ----------------------------------------------------------------- flush ---
 
 void Executor::flush(const Bits* live, int* extra) {
+  if (tracing_)
+    throw RuntimeError("batch execution needs straight-line programs: this one needs the device "
+                       "during the walk (a stream condition, or a popcount used as a loop bound, "
+                       "index or shift amount)");
   const int n_nodes = static_cast<int>(nodes_.size());
   std::vector<uint8_t> is_target(n_nodes, 0), need(n_nodes, 0);
   Segment seg;
@@ -740,6 +749,51 @@ bool Executor::int_value(int name, int64_t* v) {
   if (name < 0 || !int_def_[name]) return false;
   *v = force(ints_[name]);
   return true;
+}
+
+}  // namespace bsz
+
+// ----------------------------------------------------------------- trace ---
+
+namespace bsz {
+
+Executor::Traced Executor::trace() {
+  tracing_ = true;
+  Traced t;
+  for (int id : prog_.inputs) {
+    if (prog_.is_array[id]) throw RuntimeError("batch execution does not take input arrays");
+    int n = buf_node(nullptr, 0, false);   // symbolic input: no buffer, length-independent
+    var_[id] = n;
+    t.input_nodes.push_back(n);
+  }
+  exec_block(prog_.stmts);
+  for (int id : prog_.outputs) {
+    if (prog_.is_array[id]) throw RuntimeError("batch execution does not produce output arrays");
+    t.output_nodes.push_back(var_[id] >= 0 ? var_[id] : -1);
+  }
+  t.pops = pending_pops_;
+  std::function<void(int32_t, std::vector<std::pair<char, int64_t>>&)> post =
+      [&](int32_t e, std::vector<std::pair<char, int64_t>>& out) {
+        const IE& x = iexpr_[e];
+        if (x.op == 'k' || x.op == 's') {
+          out.push_back({x.op, x.v});
+          return;
+        }
+        post(x.a, out);
+        post(x.b, out);
+        out.push_back({x.op, 0});
+      };
+  for (int id : prog_.output_ints) {
+    std::vector<std::pair<char, int64_t>> prog;
+    const IntV& v = ints_[id];
+    if (v.e < 0) prog.push_back({'k', v.v});
+    else post(v.e, prog);
+    t.int_outputs.push_back(std::move(prog));
+  }
+  t.nodes = nodes_;
+  t.op_count = op_count;
+  tracing_ = false;
+  return t;
 }
 
 }  // namespace bsz

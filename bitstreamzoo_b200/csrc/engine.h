@@ -48,13 +48,20 @@ struct Node {
 
 enum class ExecMode : int { Plain = 0, Fused = 1 };
 
+// Fused-kernel schedule: the knobs the autotuner and the cost model choose.
+struct Schedule {
+  int warps = 4;          // warps per CTA
+  int range_steps = 64;   // minimum 32-word steps per warp range (words per tile / 32)
+  int ctas_per_sm = 0;    // resident CTAs per SM; 0 = as many as the kernel's occupancy allows
+  int min_blocks = 4;     // __launch_bounds__ minimum blocks (caps registers per thread)
+  int prefetch = 1;       // issue the next step's loads before the current step's arithmetic
+  int cut_adds = 0;       // 1: every addition ends a part (its result is materialized)
+};
+
 struct ExecOptions {
   ExecMode mode = ExecMode::Plain;
   bool simplify = false;        // algebraic folding + CSE (on in fused mode)
-  int fused_warps = 4;          // fused: warps per CTA
-  int fused_chunk_steps = 64;   // fused: 32-word steps per warp chunk
-  int fused_warmup_steps = 2;   // fused: speculative warm-up steps before a chunk
-  int fused_ctas_per_sm = 4;    // fused: grid = SMs * this (persistent)
+  Schedule sched;
 };
 
 // A segment handed to the plain or fused backend: nodes in topological order.
@@ -99,6 +106,25 @@ class Executor {
   double compile_ms = 0.0;
   int64_t fused_launches() const;
   int64_t fused_fallbacks() const;
+  void set_schedule(const Schedule& s);
+
+  // ---- batch support ----------------------------------------------------
+  // A straight-line program traced symbolically: its DAG from the declared
+  // scalar inputs to the declared scalar outputs and popcounts, independent
+  // of the stream length.  Integer outputs are postfix programs over the
+  // popcount slots: ('k', value) constant, ('s', slot), '+', '-', '*'.
+  struct Traced {
+    std::vector<Node> nodes;
+    std::vector<int> input_nodes;    // per scalar input of the program
+    std::vector<int> output_nodes;   // per scalar output stream (-1: never assigned)
+    std::vector<std::pair<int, int64_t>> pops;   // (node, slot 0..n-1)
+    std::vector<std::vector<std::pair<char, int64_t>>> int_outputs;   // per output int
+    int64_t op_count = 0;
+  };
+  // Walks the program with unbound symbolic inputs.  Throws if the program
+  // needs the device during the walk (if/while on a stream, an int from a
+  // popcount used as a loop bound, index or shift amount, arrays).
+  Traced trace();
 
  private:
   struct IntV { int64_t v = 0; int32_t e = -1; };
@@ -141,6 +167,7 @@ class Executor {
 
   std::unique_ptr<FusedBackend> fused_;
   unsigned int* d_flag_ = nullptr;
+  bool tracing_ = false;   // symbolic walk for batches: no device work, no length-dependent folds
 
   // walk
   void exec_block(const std::vector<Stmt>& v);

@@ -29,6 +29,8 @@
 
 #include <cuda.h>
 #include <nvrtc.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <chrono>
@@ -53,6 +55,7 @@ struct Driver {
   CUresult (*launch_kernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
                             unsigned, CUstream, void**, void**) = nullptr;
   CUresult (*get_error_string)(CUresult, const char**) = nullptr;
+  CUresult (*occupancy)(int*, CUfunction, int, size_t) = nullptr;
 };
 
 template <class F>
@@ -73,6 +76,7 @@ const Driver& drv() {
     resolve("cuFuncGetAttribute", x.func_get_attribute);
     resolve("cuLaunchKernel", x.launch_kernel);
     resolve("cuGetErrorString", x.get_error_string);
+    resolve("cuOccupancyMaxActiveBlocksPerMultiprocessor", x.occupancy);
     return x;
   }();
   return d;
@@ -94,6 +98,7 @@ struct Compiled {
   CUmodule mod = nullptr;
   CUfunction fn = nullptr;
   int n_regs = 0;
+  int blocks_per_sm = 1;   // occupancy of the compiled kernel at its block size
 };
 
 // Process-wide cache of compiled kernels keyed by generated source.
@@ -124,6 +129,15 @@ FusedBackend::FusedBackend(Device& dev, const ExecOptions& opt)
     : impl_(std::make_unique<Impl>(dev, opt)) {}
 FusedBackend::~FusedBackend() = default;
 
+void FusedBackend::set_schedule(const Schedule& s) {
+  Schedule c = s;
+  c.warps = std::max(1, std::min(c.warps, 16));
+  c.range_steps = std::max(1, c.range_steps);
+  c.ctas_per_sm = std::max(0, c.ctas_per_sm);
+  c.min_blocks = std::max(1, std::min(c.min_blocks, 32));
+  impl_->opt.sched = c;
+}
+
 namespace {
 
 // One kernel's worth of the segment.
@@ -141,22 +155,86 @@ struct Gen {
   int warps;
   int min_blocks;
   bool masked;
+  bool prefetch;
+  bool guard_outputs = false;      // batches: an output pointer may be null (not stored)
+  // batches: fixed argument positions (input node -> A.in index; (node, A.out index))
+  const std::map<int, int>* in_index_override = nullptr;
+  const std::vector<std::pair<int, int>>* outs_override = nullptr;
   // derived
   std::map<int, int> in_idx;       // node -> input index
-  std::map<int, int> out_idx;      // node -> output index
+  std::vector<std::pair<int, int>> outs;   // (node, output index); a node may repeat
   std::set<int> in_part;           // computed in this part
   std::set<int> shl_src;           // temporaries shifted left (need previous-step value)
   std::map<int, int> shl_ws;       // max word shift per shl source temporary
   std::vector<uint8_t> dyn;        // node dirt must be tracked during warm-up
   std::map<int, int64_t> sdh;      // static dirt (words) for nodes without add ancestors
   int64_t warm = 64;               // warm-up words
+  // Global loads of one step ("load slots"): expression templates over @W@
+  // (this lane's word) and @B@ (the step's first word), de-duplicated.  The
+  // owned-range loop issues them one step ahead of the arithmetic.
+  std::vector<std::string> slot_tmpl;
+  std::map<std::string, int> slot_of;
 
   std::string v(int n) const { return "v" + std::to_string(n); }
   bool is_input(int n) const { return in_idx.count(n) != 0; }
 
+  int slot(const std::string& tmpl) {
+    auto it = slot_of.find(tmpl);
+    if (it != slot_of.end()) return it->second;
+    int id = static_cast<int>(slot_tmpl.size());
+    slot_tmpl.push_back(tmpl);
+    slot_of[tmpl] = id;
+    return id;
+  }
+  static std::string subst(std::string t, const std::string& w, const std::string& b) {
+    for (size_t p; (p = t.find("@W@")) != std::string::npos;) t.replace(p, 3, w);
+    for (size_t p; (p = t.find("@B@")) != std::string::npos;) t.replace(p, 3, b);
+    return t;
+  }
+  std::string slot_cur(const std::string& tmpl) const { return "cur" + std::to_string(slot_of.at(tmpl)); }
+  // templates used by nodes
+  std::string t_word(int n) const { return load(n, "@W@"); }
+  std::string t_shl_lo(const Node& x) const { return load(x.a, "@W@ - " + std::to_string(x.k / 64) + "ll"); }
+  std::string t_shl_edge(const Node& x) const {
+    return "(lane == 0 ? " + load(x.a, "@B@ - " + std::to_string(x.k / 64 + 1) + "ll") + " : 0ull)";
+  }
+  std::string t_shr_lo(const Node& x) const { return load(x.a, "@W@ + " + std::to_string(x.k / 64) + "ll"); }
+  std::string t_shr_edge(const Node& x) const {
+    return "(lane == 31 ? " + load(x.a, "@B@ + " + std::to_string(x.k / 64 + 32) + "ll") + " : 0ull)";
+  }
+  void make_slots() {
+    for (auto& kv : in_idx) slot(t_word(kv.first));
+    for (int n : part.order) {
+      const Node& x = nodes[n];
+      if (x.op == NOp::Shl && (is_input(x.a) || is_const(nodes[x.a].op))) {
+        slot(t_shl_lo(x));
+        if (x.k % 64) slot(t_shl_edge(x));
+      } else if (x.op == NOp::Shr) {
+        slot(t_shr_lo(x));
+        if (x.k % 64) slot(t_shr_edge(x));
+      }
+    }
+  }
+  // assignments of every load slot for the step starting at `b` (lane word `w`)
+  void emit_loads(std::ostringstream& s, const std::string& prefix, bool declare, const std::string& w,
+                  const std::string& b, const char* indent) const {
+    for (size_t i = 0; i < slot_tmpl.size(); ++i)
+      s << indent << (declare ? "const u64 " : "") << prefix << i << " = " << subst(slot_tmpl[i], w, b)
+        << ";\n";
+  }
+
   void analyze() {
-    for (size_t i = 0; i < part.inputs.size(); ++i) in_idx[part.inputs[i]] = static_cast<int>(i);
-    for (size_t i = 0; i < part.outputs.size(); ++i) out_idx[part.outputs[i]] = static_cast<int>(i);
+    if (in_index_override) {
+      for (int n : part.inputs) {
+        auto it = in_index_override->find(n);
+        in_idx[n] = it == in_index_override->end() ? 0 : it->second;   // constants: index unused
+      }
+    } else {
+      for (size_t i = 0; i < part.inputs.size(); ++i) in_idx[part.inputs[i]] = static_cast<int>(i);
+    }
+    if (outs_override) outs = *outs_override;
+    else
+      for (size_t i = 0; i < part.outputs.size(); ++i) outs.push_back({part.outputs[i], static_cast<int>(i)});
     for (int n : part.order) in_part.insert(n);
     dyn.assign(nodes.size(), 0);
     int64_t max_static = 0;
@@ -182,15 +260,19 @@ struct Gen {
     }
     warm = ((max_static + 64 + 31) / 32) * 32;
     if (warm > 8192) warm = 8192;
+    make_slots();
   }
 
   // expression for an input node value at word index expression `idx`
   std::string load(int n, const std::string& idx) const {
+    // Word `idx` of a stream; words below 0 are zero (shifting in zeros),
+    // words at or past nw are the tail.
     const Node& x = nodes[n];
     if (x.op == NOp::Zero) return "0ull";
-    if (x.op == NOp::AllOnes) return "~0ull";
+    if (x.op == NOp::AllOnes) return "((" + idx + ") >= 0 ? ~0ull : 0ull)";
     if (x.op == NOp::OnesMask)
-      return "((" + idx + ") < A.nw - 1 ? ~0ull : ((" + idx + ") == A.nw - 1 ? A.last_mask : 0ull))";
+      return "((" + idx + ") >= 0 && (" + idx + ") < A.nw - 1 ? ~0ull : ((" + idx +
+             ") == A.nw - 1 ? A.last_mask : 0ull))";
     std::string fill = x.tail ? "~0ull" : "0ull";
     return "((" + idx + ") >= 0 && (" + idx + ") < A.nw ? __ldg(A.in[" + std::to_string(in_idx.at(n)) +
            "] + (" + idx + ")) : " + fill + ")";
@@ -199,14 +281,13 @@ struct Gen {
   // value of operand o in the current step (already computed or loaded)
   std::string opnd(int o) const { return v(o); }
 
-  void emit_step(std::ostringstream& s, bool track) const {
+  // One 32-word step.  prefetched: the load slots are already in cur<i>
+  // (the owned-range loop loads them a step ahead); otherwise load here.
+  void emit_step(std::ostringstream& s, bool track, bool prefetched) const {
     s << "      const long long w = base + lane;\n";
     if (masked) s << "      const u64 lm = (w == A.nw - 1) ? A.last_mask : ~0ull;\n";
-    // loads of unshifted inputs
-    for (auto& kv : in_idx) {
-      int n = kv.first;
-      s << "      const u64 " << v(n) << " = " << load(n, "w") << ";\n";
-    }
+    if (!prefetched) emit_loads(s, "cur", true, "w", "base", "      ");
+    for (auto& kv : in_idx) s << "      const u64 " << v(kv.first) << " = " << slot_cur(t_word(kv.first)) << ";\n";
     if (track) s << "      const int rel = (int)(base - p0);\n";
     for (int n : part.order) {
       const Node& x = nodes[n];
@@ -248,11 +329,10 @@ struct Gen {
           int bs = static_cast<int>(x.k % 64);
           if (is_input(x.a) || is_const(nodes[x.a].op)) {
             s << "      u64 " << v(n) << ";\n      {\n"
-              << "        const u64 lo = " << load(x.a, "w - " + std::to_string(ws) + "ll") << ";\n";
+              << "        const u64 lo = " << slot_cur(t_shl_lo(x)) << ";\n";
             if (bs) {
               s << "        u64 hi = __shfl_up_sync(~0u, lo, 1);\n"
-                << "        if (lane == 0) hi = " << load(x.a, "base - " + std::to_string(ws + 1) + "ll")
-                << ";\n"
+                << "        if (lane == 0) hi = " << slot_cur(t_shl_edge(x)) << ";\n"
                 << "        " << v(n) << " = (lo << " << bs << ") | (hi >> " << (64 - bs) << ");\n";
             } else {
               s << "        " << v(n) << " = lo;\n";
@@ -286,13 +366,12 @@ struct Gen {
         }
         case NOp::Shr: {
           // only inputs reach here (temporaries are cut)
-          int64_t ws = x.k / 64;
           int bs = static_cast<int>(x.k % 64);
           s << "      u64 " << v(n) << ";\n      {\n"
-            << "        const u64 lo = " << load(x.a, "w + " + std::to_string(ws) + "ll") << ";\n";
+            << "        const u64 lo = " << slot_cur(t_shr_lo(x)) << ";\n";
           if (bs) {
             s << "        u64 hi = __shfl_down_sync(~0u, lo, 1);\n"
-              << "        if (lane == 31) hi = " << load(x.a, "base + " + std::to_string(ws + 32) + "ll") << ";\n"
+              << "        if (lane == 31) hi = " << slot_cur(t_shr_edge(x)) << ";\n"
               << "        " << v(n) << " = (lo >> " << bs << ") | (hi << " << (64 - bs) << ");\n";
           } else {
             s << "        " << v(n) << " = lo;\n";
@@ -319,7 +398,9 @@ struct Gen {
     for (int n : shl_src) s << "      pv" << n << " = " << v(n) << ";\n";
     if (!track) {
       s << "      if (w < e) {\n";
-      for (auto& kv : out_idx) s << "        A.out[" << kv.second << "][w] = " << v(kv.first) << ";\n";
+      for (auto& kv : outs)
+        s << "        " << (guard_outputs ? "if (A.out[" + std::to_string(kv.second) + "]) " : std::string())
+          << "A.out[" << kv.second << "][w] = " << v(kv.first) << ";\n";
       for (size_t j = 0; j < part.pops.size(); ++j)
         s << "        pc" << j << " += __popcll(" << v(part.pops[j].first) << ");\n";
       s << "      }\n";
@@ -335,14 +416,21 @@ struct Gen {
     return std::to_string(it == sdh.end() ? 0 : it->second);
   }
 
+  static std::string args_struct(int ni, int no) {
+    std::ostringstream s;
+    s << "typedef unsigned long long u64;\ntypedef unsigned int u32;\n"
+      << "struct Args {\n  const u64* in[" << std::max(1, ni) << "];\n  u64* out[" << std::max(1, no)
+      << "];\n  unsigned long long* slots;\n  unsigned int* fail;\n  long long nw;\n"
+      << "  long long range;\n  u64 last_mask;\n};\n";
+    return s.str();
+  }
+
+  // Whole kernel for one segment part: each warp owns range [s, e).
   std::string source() {
     analyze();
     std::ostringstream s;
     const int ni = static_cast<int>(part.inputs.size()), no = static_cast<int>(part.outputs.size());
-    s << "typedef unsigned long long u64;\ntypedef unsigned int u32;\n"
-      << "struct Args {\n  const u64* in[" << std::max(1, ni) << "];\n  u64* out[" << std::max(1, no)
-      << "];\n  unsigned long long* slots;\n  unsigned int* fail;\n  long long nw;\n"
-      << "  long long range;\n  u64 last_mask;\n};\n"
+    s << args_struct(ni, no)
       << "extern \"C\" __global__ void __launch_bounds__(" << warps * 32 << ", " << min_blocks
       << ")\nbsz_fused(const Args A) {\n"
       << "  const int lane = threadIdx.x & 31;\n"
@@ -350,6 +438,24 @@ struct Gen {
       << "  const long long s = gw * A.range;\n"
       << "  if (s >= A.nw) return;\n"
       << "  const long long e = min(s + A.range, A.nw);\n";
+    body(s);
+    s << "}\n";
+    return s.str();
+  }
+
+  // Device function for batches: one work item = range [s, e) of one instance.
+  std::string device_function(const std::string& name) {
+    analyze();
+    std::ostringstream s;
+    s << "__device__ __noinline__ void " << name
+      << "(const Args& Ap, const long long s, const long long e, const int lane) {\n"
+      << "  const Args A = Ap;\n";
+    body(s);
+    s << "}\n";
+    return s.str();
+  }
+
+  void body(std::ostringstream& s) {
     std::vector<int> adds;
     for (int n : part.order)
       if (nodes[n].op == NOp::Add) adds.push_back(n);
@@ -369,7 +475,7 @@ struct Gen {
       for (int n : part.order)
         if (dyn[n] && nodes[n].op != NOp::Add) s << "    int dh" << n << " = 0;\n";
       s << "    for (long long base = p0; base < s; base += 32) {\n";
-      emit_step(s, true);
+      emit_step(s, true, false);
       s << "    }\n";
       // exactness: every carry and every previous-step value at s is exact
       s << "    const int need = (int)(s - p0);\n    bool ok = true;\n";
@@ -385,21 +491,101 @@ struct Gen {
         << "    p0 = s - 2 * (s - p0);\n    if (p0 < 0) p0 = 0;\n"
         << "  }\n";
     }
-    // ---- owned range
-    s << "  for (long long base = s; base < e; base += 32) {\n";
-    emit_step(s, false);
+    // ---- owned range: the loads of step t+1 are issued before the arithmetic
+    // of step t, so each warp keeps two steps of loads in flight.
+    if (!prefetch) {
+      s << "  for (long long base = s; base < e; base += 32) {\n";
+      emit_step(s, false, false);
+      s << "  }\n";
+    } else {
+    for (size_t i = 0; i < slot_tmpl.size(); ++i) s << "  u64 pf" << i << ";\n";
+    s << "  {\n    const long long base = s;\n    const long long w = base + lane;\n";
+    emit_loads(s, "pf", false, "w", "base", "    ");
     s << "  }\n";
+    s << "  for (long long base = s; base < e; base += 32) {\n";
+    for (size_t i = 0; i < slot_tmpl.size(); ++i) s << "      const u64 cur" << i << " = pf" << i << ";\n";
+    s << "      {\n        const long long bn = base + 32;\n        if (bn < e) {\n"
+      << "          const long long wn = bn + lane;\n";
+    emit_loads(s, "pf", false, "wn", "bn", "          ");
+    s << "        }\n      }\n";
+    emit_step(s, false, true);
+    s << "  }\n";
+    }
     for (size_t j = 0; j < part.pops.size(); ++j) {
       s << "  {\n    unsigned long long t = pc" << j << ";\n"
         << "    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(~0u, t, o);\n"
         << "    if (lane == 0 && t) atomicAdd(A.slots + " << part.pops[j].second << ", t);\n  }\n";
     }
-    s << "}\n";
-    return s.str();
   }
 };
 
-Compiled compile_source(const std::string& src, double* compile_ms) {
+// On-disk cache of compiled kernels, so that short-lived processes (the
+// bsim_cuda driver runs once per test case) do not recompile: directory
+// $BSZ_KERNEL_CACHE (or ~/.cache/bitstreamzoo_b200; "off" disables), files
+// <hash>.cubin next to <hash>.cu holding the full source, which is compared
+// on load so a hash collision can never return the wrong kernel.
+std::string cache_dir() {
+  const char* env = std::getenv("BSZ_KERNEL_CACHE");
+  if (env && !std::strcmp(env, "off")) return "";
+  std::string d;
+  if (env && *env) d = env;
+  else if (const char* home = std::getenv("HOME")) d = std::string(home) + "/.cache/bitstreamzoo_b200";
+  else return "";
+  std::string cur;
+  for (size_t i = 0; i <= d.size(); ++i) {   // mkdir -p
+    if (i == d.size() || d[i] == '/') {
+      if (!cur.empty()) mkdir(cur.c_str(), 0755);
+    }
+    if (i < d.size()) cur += d[i];
+  }
+  return d;
+}
+
+std::string cache_key(const std::string& src) {
+  uint64_t h = 1469598103934665603ull;   // FNV-1a over the source and the target
+  for (char c : src + "|sm_100a|nvrtc-12") h = (h ^ static_cast<unsigned char>(c)) * 1099511628211ull;
+  char buf[32];
+  std::snprintf(buf, sizeof buf, "%016llx", static_cast<unsigned long long>(h));
+  return buf;
+}
+
+std::string read_file(const std::string& path) {
+  std::string out;
+  if (FILE* f = std::fopen(path.c_str(), "rb")) {
+    char buf[1 << 16];
+    size_t n;
+    while ((n = std::fread(buf, 1, sizeof buf, f)) > 0) out.append(buf, n);
+    std::fclose(f);
+  }
+  return out;
+}
+
+std::string disk_cache_load(const std::string& src) {
+  const std::string dir = cache_dir();
+  if (dir.empty()) return "";
+  const std::string base = dir + "/" + cache_key(src);
+  if (read_file(base + ".cu") != src) return "";
+  return read_file(base + ".cubin");
+}
+
+void disk_cache_store(const std::string& src, const std::string& cubin) {
+  const std::string dir = cache_dir();
+  if (dir.empty()) return;
+  const std::string base = dir + "/" + cache_key(src);
+  const std::string tag = "." + std::to_string(getpid());
+  for (const auto& [ext, data] : {std::pair<std::string, const std::string*>{".cubin", &cubin},
+                                  {".cu", &src}}) {
+    const std::string tmp = base + ext + tag;
+    if (FILE* f = std::fopen(tmp.c_str(), "wb")) {
+      std::fwrite(data->data(), 1, data->size(), f);
+      std::fclose(f);
+      std::rename(tmp.c_str(), (base + ext).c_str());
+    }
+  }
+}
+
+Compiled compile_source(const std::string& src, int block_threads, double* compile_ms,
+                        const char* kernel = "bsz_fused") {
   {
     std::lock_guard<std::mutex> lk(g_cache_mu);
     auto it = cache().find(src);
@@ -415,30 +601,36 @@ Compiled compile_source(const std::string& src, double* compile_ms) {
       std::fclose(f);
     }
   }
-  nvrtcProgram prog;
-  if (nvrtcCreateProgram(&prog, src.c_str(), "bsz_fused.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
-    throw RuntimeError("nvrtcCreateProgram failed");
   // warnings 550/177: warm-up steps compute values only the owned range stores
   const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-default-device",
                         "--extra-device-vectorization", "--diag-suppress=550,177"};
-  nvrtcResult r = nvrtcCompileProgram(prog, 5, opts);
-  if (r != NVRTC_SUCCESS) {
-    size_t n = 0;
-    nvrtcGetProgramLogSize(prog, &n);
-    std::string log(n, '\0');
-    nvrtcGetProgramLog(prog, &log[0]);
+  std::string cubin = disk_cache_load(src);
+  if (cubin.empty()) {
+    nvrtcProgram prog;
+    if (nvrtcCreateProgram(&prog, src.c_str(), "bsz_fused.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
+      throw RuntimeError("nvrtcCreateProgram failed");
+    nvrtcResult r = nvrtcCompileProgram(prog, 5, opts);
+    if (r != NVRTC_SUCCESS) {
+      size_t n = 0;
+      nvrtcGetProgramLogSize(prog, &n);
+      std::string log(n, '\0');
+      nvrtcGetProgramLog(prog, &log[0]);
+      nvrtcDestroyProgram(&prog);
+      throw RuntimeError("NVRTC compile failed: " + log.substr(0, 2000));
+    }
+    size_t cubin_size = 0;
+    nvrtcGetCUBINSize(prog, &cubin_size);
+    cubin.assign(cubin_size, '\0');
+    nvrtcGetCUBIN(prog, &cubin[0]);
     nvrtcDestroyProgram(&prog);
-    throw RuntimeError("NVRTC compile failed: " + log.substr(0, 2000));
+    disk_cache_store(src, cubin);
   }
-  size_t cubin_size = 0;
-  nvrtcGetCUBINSize(prog, &cubin_size);
-  std::string cubin(cubin_size, '\0');
-  nvrtcGetCUBIN(prog, &cubin[0]);
-  nvrtcDestroyProgram(&prog);
   Compiled c;
   BSZ_CU(drv().module_load_data(&c.mod, cubin.data()));
-  BSZ_CU(drv().module_get_function(&c.fn, c.mod, "bsz_fused"));
+  BSZ_CU(drv().module_get_function(&c.fn, c.mod, kernel));
   drv().func_get_attribute(&c.n_regs, CU_FUNC_ATTRIBUTE_NUM_REGS, c.fn);
+  if (drv().occupancy(&c.blocks_per_sm, c.fn, block_threads, 0) != CUDA_SUCCESS || c.blocks_per_sm < 1)
+    c.blocks_per_sm = 1;
   if (compile_ms)
     *compile_ms += std::chrono::duration<double, std::milli>(std::chrono::high_resolution_clock::now() - t0).count();
   std::lock_guard<std::mutex> lk(g_cache_mu);
@@ -449,7 +641,7 @@ Compiled compile_source(const std::string& src, double* compile_ms) {
 // Splits a segment into parts: a node that reads a temporary through a right
 // shift, or through a left shift of 2048 bits or more, starts a later part,
 // and that temporary becomes an output of its own part.
-std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg) {
+std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg, bool cut_adds) {
   std::map<int, int> level;
   std::set<int> computed(seg.order.begin(), seg.order.end());
   std::set<int> cut_src;
@@ -459,7 +651,8 @@ std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg) {
     for (int o : {x.a, x.b}) {
       if (o < 0 || !computed.count(o)) continue;
       int l = level[o];
-      bool cut = (x.op == NOp::Shr) || (x.op == NOp::Shl && x.k / 64 >= 32);
+      bool cut = (x.op == NOp::Shr) || (x.op == NOp::Shl && x.k / 64 >= 32) ||
+                 (cut_adds && nodes[o].op == NOp::Add);
       if (cut) {
         cut_src.insert(o);
         l += 1;
@@ -511,13 +704,14 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
                        unsigned long long* d_slots, double* compile_ms) {
   Device& dev = impl_->dev;
   const ExecOptions& opt = impl_->opt;
-  std::vector<Part> parts = split(nodes, seg);
+  const Schedule& sc = opt.sched;
+  std::vector<Part> parts = split(nodes, seg, sc.cut_adds != 0);
   for (Part& p : parts) {
     if (p.order.empty() && p.pops.empty()) continue;
     if (p.inputs.size() > kMaxInputs) throw RuntimeError("fused: too many inputs in one segment");
-    Gen g{nodes, p, N, opt.fused_warps, opt.fused_ctas_per_sm, (N % 64) != 0};
+    Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
     const std::string src = g.source();
-    Compiled c = compile_source(src, compile_ms);
+    Compiled c = compile_source(src, sc.warps * 32, compile_ms);
     // outputs
     for (int n : p.outputs)
       if (!nodes[n].buf) nodes[n].buf = dev.alloc_stream(nw);
@@ -532,12 +726,14 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
     for (size_t i = 0; i < p.outputs.size(); ++i) args[ni + i] = reinterpret_cast<uint64_t>(nodes[p.outputs[i]].buf->p);
     // grid: contiguous ranges of whole 32-word steps, at least 8 warm-ups long
     const int64_t steps = (nw + 31) / 32;
-    int64_t max_warps = static_cast<int64_t>(dev.sm_count()) * opt.fused_ctas_per_sm * opt.fused_warps;
-    int64_t min_range_steps = std::max<int64_t>(opt.fused_chunk_steps, (g.warm / 32) * 8);
+    // persistent grid: as many warps as the compiled kernel keeps resident
+    const int per_sm = sc.ctas_per_sm > 0 ? std::min(sc.ctas_per_sm, c.blocks_per_sm) : c.blocks_per_sm;
+    int64_t max_warps = static_cast<int64_t>(dev.sm_count()) * per_sm * sc.warps;
+    int64_t min_range_steps = std::max<int64_t>(sc.range_steps, (g.warm / 32) * 8);
     int64_t warps_needed = std::max<int64_t>(1, std::min(max_warps, (steps + min_range_steps - 1) / min_range_steps));
     int64_t range = ((steps + warps_needed - 1) / warps_needed) * 32;
     int64_t total_warps = (nw + range - 1) / range;
-    int blocks = static_cast<int>((total_warps + opt.fused_warps - 1) / opt.fused_warps);
+    int blocks = static_cast<int>((total_warps + sc.warps - 1) / sc.warps);
     args[ni + no + 0] = reinterpret_cast<uint64_t>(d_slots);
     args[ni + no + 1] = reinterpret_cast<uint64_t>(impl_->d_fail);
     args[ni + no + 2] = static_cast<uint64_t>(nw);
@@ -547,7 +743,7 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
     void* kparams[] = {args.data()};
     {
       ProfScope prof(dev, "fused");
-      BSZ_CU(drv().launch_kernel(c.fn, blocks, 1, 1, opt.fused_warps * 32, 1, 1, 0,
+      BSZ_CU(drv().launch_kernel(c.fn, blocks, 1, 1, sc.warps * 32, 1, 1, 0,
                             reinterpret_cast<CUstream>(dev.stream()), kparams, nullptr));
     }
     ++dev.n_launches;
@@ -607,6 +803,301 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
       ++fallbacks;
     }
   }
+}
+
+// ================================================================ batches ==
+
+namespace {
+
+struct BatchProg {
+  Executor::Traced t;
+  Part part;
+  std::map<int, int> in_index;
+  std::vector<std::pair<int, int>> outs;
+  std::string fn;
+  int64_t warm = 64;
+};
+
+struct BatchItem {   // layout shared with the generated kernel's Item
+  int32_t inst;
+  int32_t dag;
+  int64_t s;
+  int64_t e;
+};
+
+int64_t eval_postfix(const std::vector<std::pair<char, int64_t>>& prog, const uint64_t* slots) {
+  std::vector<int64_t> st;
+  for (const auto& op : prog) {
+    if (op.first == 'k') {
+      st.push_back(op.second);
+    } else if (op.first == 's') {
+      st.push_back(static_cast<int64_t>(slots[op.second]));
+    } else {
+      int64_t b = st.back();
+      st.pop_back();
+      int64_t a = st.back();
+      st.pop_back();
+      st.push_back(op.first == '+' ? a + b : op.first == '-' ? a - b : a * b);
+    }
+  }
+  return st.empty() ? 0 : st.back();
+}
+
+// Builds the single part of a traced straight-line program.
+void plan_batch_program(BatchProg& bp) {
+  const Executor::Traced& t = bp.t;
+  const auto& nodes = t.nodes;
+  std::vector<uint8_t> need(nodes.size(), 0);
+  std::vector<int> stack;
+  for (int n : t.output_nodes)
+    if (n >= 0) stack.push_back(n);
+  for (auto& p : t.pops) stack.push_back(p.first);
+  auto computed = [&](int n) {
+    NOp op = nodes[n].op;
+    return op != NOp::Buf && op != NOp::Zero && op != NOp::OnesMask && op != NOp::AllOnes;
+  };
+  while (!stack.empty()) {
+    int n = stack.back();
+    stack.pop_back();
+    if (need[n]) continue;
+    need[n] = 1;
+    if (!computed(n)) continue;
+    for (int o : {nodes[n].a, nodes[n].b})
+      if (o >= 0) stack.push_back(o);
+  }
+  for (size_t n = 0; n < nodes.size(); ++n) {
+    if (!need[n]) continue;
+    if (computed(static_cast<int>(n))) {
+      const Node& x = nodes[n];
+      if (x.op == NOp::Shr && computed(x.a))
+        throw RuntimeError("batch: a right shift of a temporary is not supported in batches");
+      if (x.op == NOp::Shl && computed(x.a) && x.k / 64 >= 32)
+        throw RuntimeError("batch: a left shift of a temporary by 2048 bits or more is not supported");
+      bp.part.order.push_back(static_cast<int>(n));
+    } else {
+      bp.part.inputs.push_back(static_cast<int>(n));
+    }
+  }
+  for (size_t i = 0; i < t.input_nodes.size(); ++i) bp.in_index[t.input_nodes[i]] = static_cast<int>(i);
+  for (size_t j = 0; j < t.output_nodes.size(); ++j)
+    if (t.output_nodes[j] >= 0) bp.outs.push_back({t.output_nodes[j], static_cast<int>(j)});
+  bp.part.pops = t.pops;
+}
+
+}  // namespace
+
+struct BatchRunner::Impl {
+  Device& dev;
+  Schedule sched;
+  std::vector<BatchProg> progs;
+  std::vector<const Program*> srcs;
+  std::vector<BatchInstance> inst;
+  std::vector<int64_t> slot_base;
+  int64_t n_slots = 0;
+  int64_t n_items = 0;
+  int max_in = 1, max_out = 1;
+  Compiled kern;
+  void* d_args = nullptr;
+  void* d_items = nullptr;
+  unsigned long long* d_slots = nullptr;
+  unsigned int* d_ctrl = nullptr;   // [0] work counter, [1] speculation-failed flag
+  int blocks = 1;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<uint64_t> h_slots;
+  std::vector<std::vector<int64_t>> ints;
+  explicit Impl(Device& d) : dev(d) {}
+  ~Impl() {
+    cudaStreamSynchronize(dev.stream());
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (void* p : {d_args, d_items, static_cast<void*>(d_slots), static_cast<void*>(d_ctrl)})
+      if (p) cudaFree(p);
+  }
+  void* upload(const void* host, size_t bytes) {
+    void* p = nullptr;
+    BSZ_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 256)));
+    ++dev.n_mallocs;
+    if (bytes) BSZ_CUDA(cudaMemcpyAsync(p, host, bytes, cudaMemcpyHostToDevice, dev.stream()));
+    return p;
+  }
+};
+
+BatchRunner::BatchRunner(Device& dev, const std::vector<const Program*>& progs,
+                         std::vector<BatchInstance> instances, const Schedule& sched)
+    : impl_(std::make_unique<Impl>(dev)) {
+  Impl& m = *impl_;
+  m.sched = sched;
+  m.srcs = progs;
+  m.inst = std::move(instances);
+  // 1. trace every program symbolically and plan its DAG
+  ExecOptions eo;
+  eo.mode = ExecMode::Fused;
+  eo.sched = sched;
+  std::string fns;
+  for (size_t k = 0; k < progs.size(); ++k) {
+    BatchProg bp;
+    {
+      Executor ex(dev, *progs[k], int64_t(1) << 20, eo);
+      bp.t = ex.trace();
+    }
+    plan_batch_program(bp);
+    Gen g{bp.t.nodes, bp.part, 0, sched.warps, sched.min_blocks, true, sched.prefetch != 0};
+    g.guard_outputs = true;
+    g.in_index_override = &bp.in_index;
+    g.outs_override = &bp.outs;
+    bp.fn = g.device_function("dag_" + std::to_string(k));
+    bp.warm = g.warm;
+    m.max_in = std::max<int>(m.max_in, static_cast<int>(bp.t.input_nodes.size()));
+    m.max_out = std::max<int>(m.max_out, static_cast<int>(bp.t.output_nodes.size()));
+    fns += bp.fn;
+    m.progs.push_back(std::move(bp));
+  }
+  // 2. one kernel: every program's DAG as a device function + a work loop
+  std::ostringstream src;
+  src << Gen::args_struct(m.max_in, m.max_out) << fns
+      << "struct Item { int inst; int dag; long long s; long long e; };\n"
+      << "extern \"C\" __global__ void __launch_bounds__(" << sched.warps * 32 << ", "
+      << sched.min_blocks << ")\nbsz_batch(const Args* __restrict__ insts, "
+      << "const Item* __restrict__ items, const long long n_items, unsigned int* __restrict__ ctrl) {\n"
+      << "  const int lane = threadIdx.x & 31;\n"
+      << "  for (;;) {\n"
+      << "    unsigned int it = 0;\n"
+      << "    if (lane == 0) it = atomicAdd(ctrl, 1u);\n"
+      << "    it = __shfl_sync(~0u, it, 0);\n"
+      << "    if (it >= n_items) return;\n"
+      << "    const Item I = items[it];\n"
+      << "    switch (I.dag) {\n";
+  for (size_t k = 0; k < m.progs.size(); ++k)
+    src << "      case " << k << ": dag_" << k << "(insts[I.inst], I.s, I.e, lane); break;\n";
+  src << "      default: break;\n    }\n  }\n}\n";
+  m.kern = compile_source(src.str(), sched.warps * 32, &compile_ms, "bsz_batch");
+  // 3. argument blocks (one Args per instance), slots and work items
+  const size_t stride = static_cast<size_t>(m.max_in + m.max_out + 5);
+  std::vector<uint64_t> args(stride * m.inst.size(), 0);
+  BSZ_CUDA(cudaMalloc(&m.d_ctrl, 256));
+  ++dev.n_mallocs;
+  std::vector<BatchItem> items;
+  for (size_t i = 0; i < m.inst.size(); ++i) {
+    const BatchInstance& bi = m.inst[i];
+    if (bi.program < 0 || bi.program >= static_cast<int>(m.progs.size()))
+      throw std::invalid_argument("batch: instance program index out of range");
+    const BatchProg& bp = m.progs[bi.program];
+    if (bi.inputs.size() != bp.t.input_nodes.size() || bi.outputs.size() != bp.t.output_nodes.size())
+      throw std::invalid_argument("batch: instance " + std::to_string(i) +
+                                  " does not give one pointer per declared input/output stream");
+    m.slot_base.push_back(m.n_slots);
+    m.n_slots += static_cast<int64_t>(bp.t.pops.size());
+    const int64_t nw = std::max<int64_t>(1, (bi.bitlength + 63) / 64);
+    const int64_t range = 32 * std::max<int64_t>(sched.range_steps, (bp.warm / 32) * 8);
+    for (int64_t s0 = 0; s0 < nw; s0 += range)
+      items.push_back({static_cast<int32_t>(i), bi.program, s0, std::min(nw, s0 + range)});
+    uint64_t* a = args.data() + stride * i;
+    for (size_t j = 0; j < bi.inputs.size(); ++j) a[j] = reinterpret_cast<uint64_t>(bi.inputs[j]);
+    for (size_t j = 0; j < bi.outputs.size(); ++j) a[m.max_in + j] = reinterpret_cast<uint64_t>(bi.outputs[j]);
+    a[m.max_in + m.max_out + 1] = reinterpret_cast<uint64_t>(m.d_ctrl + 1);
+    a[m.max_in + m.max_out + 2] = static_cast<uint64_t>(nw);
+    a[m.max_in + m.max_out + 3] = static_cast<uint64_t>(range);
+    a[m.max_in + m.max_out + 4] = mask_for_bits(bi.bitlength > 0 ? bi.bitlength : 64 * nw);
+  }
+  // longest items first: the atomic work queue then balances the tail
+  std::stable_sort(items.begin(), items.end(),
+                   [](const BatchItem& x, const BatchItem& y) { return (x.e - x.s) > (y.e - y.s); });
+  m.n_items = static_cast<int64_t>(items.size());
+  BSZ_CUDA(cudaMalloc(&m.d_slots, static_cast<size_t>(std::max<int64_t>(m.n_slots, 1)) * 8));
+  ++dev.n_mallocs;
+  for (size_t i = 0; i < m.inst.size(); ++i)
+    args[stride * i + m.max_in + m.max_out] = reinterpret_cast<uint64_t>(m.d_slots + m.slot_base[i]);
+  m.d_args = m.upload(args.data(), args.size() * 8);
+  m.d_items = m.upload(items.data(), items.size() * sizeof(BatchItem));
+  const int64_t per_sm = sched.ctas_per_sm > 0 ? std::min(sched.ctas_per_sm, m.kern.blocks_per_sm)
+                                               : m.kern.blocks_per_sm;
+  const int64_t want = (m.n_items + sched.warps - 1) / sched.warps;
+  m.blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(want, dev.sm_count() * per_sm)));
+  // 4. capture: reset the counters and slots, launch; replayed by launch()
+  BSZ_CUDA(cudaStreamSynchronize(dev.stream()));
+  BSZ_CUDA(cudaStreamBeginCapture(dev.stream(), cudaStreamCaptureModeThreadLocal));
+  BSZ_CUDA(cudaMemsetAsync(m.d_ctrl, 0, 8, dev.stream()));
+  BSZ_CUDA(cudaMemsetAsync(m.d_slots, 0, static_cast<size_t>(std::max<int64_t>(m.n_slots, 1)) * 8,
+                           dev.stream()));
+  long long n_items_arg = m.n_items;
+  void* kp[] = {&m.d_args, &m.d_items, &n_items_arg, &m.d_ctrl};
+  BSZ_CU(drv().launch_kernel(m.kern.fn, m.blocks, 1, 1, sched.warps * 32, 1, 1, 0,
+                             reinterpret_cast<CUstream>(dev.stream()), kp, nullptr));
+  BSZ_CUDA(cudaStreamEndCapture(dev.stream(), &m.graph));
+  BSZ_CUDA(cudaGraphInstantiate(&m.exec, m.graph, 0));
+  m.ints.assign(m.inst.size(), {});
+}
+
+BatchRunner::~BatchRunner() = default;
+
+int64_t BatchRunner::n_items() const { return impl_->n_items; }
+
+void BatchRunner::launch() {
+  Impl& m = *impl_;
+  ProfScope prof(m.dev, "bsz_batch");
+  BSZ_CUDA(cudaGraphLaunch(m.exec, m.dev.stream()));
+  ++m.dev.n_launches;
+  ++launches;
+}
+
+void BatchRunner::finish() {
+  Impl& m = *impl_;
+  unsigned int fail = 0;
+  m.h_slots.assign(static_cast<size_t>(std::max<int64_t>(m.n_slots, 1)), 0);
+  BSZ_CUDA(cudaMemcpyAsync(&fail, m.d_ctrl + 1, 4, cudaMemcpyDeviceToHost, m.dev.stream()));
+  BSZ_CUDA(cudaMemcpyAsync(m.h_slots.data(), m.d_slots, m.h_slots.size() * 8, cudaMemcpyDeviceToHost,
+                           m.dev.stream()));
+  BSZ_CUDA(cudaStreamSynchronize(m.dev.stream()));
+  if (fail) {
+    // Speculation unproven somewhere: recompute every instance with the
+    // exact per-op kernels (rare; correctness first).
+    ++fallbacks;
+    for (size_t i = 0; i < m.inst.size(); ++i) {
+      const BatchInstance& bi = m.inst[i];
+      const Program& prog = *m.srcs[bi.program];
+      const int64_t nw = std::max<int64_t>(1, (bi.bitlength + 63) / 64);
+      ExecOptions eo;
+      eo.mode = ExecMode::Plain;
+      Executor ex(m.dev, prog, bi.bitlength, eo);
+      size_t j = 0;
+      for (int id : prog.inputs) {
+        auto b = std::make_shared<DevStream>();
+        b->p = const_cast<uint64_t*>(bi.inputs[j++]);
+        b->n_words = nw;
+        ex.bind_input(id, b, 0, false);
+      }
+      ex.run();
+      j = 0;
+      for (int id : prog.outputs) {
+        uint64_t* dst = bi.outputs[j++];
+        if (dst && ex.has_stream(id))
+          BSZ_CUDA(cudaMemcpyAsync(dst, ex.stream_value(id)->p, nw * 8, cudaMemcpyDeviceToDevice,
+                                   m.dev.stream()));
+      }
+      std::vector<int64_t> v;
+      for (int id : prog.output_ints) {
+        int64_t x = 0;
+        ex.int_value(id, &x);
+        v.push_back(x);
+      }
+      m.ints[i] = std::move(v);
+    }
+    BSZ_CUDA(cudaStreamSynchronize(m.dev.stream()));
+    return;
+  }
+  for (size_t i = 0; i < m.inst.size(); ++i) {
+    const BatchProg& bp = m.progs[m.inst[i].program];
+    std::vector<int64_t> v;
+    for (const auto& post : bp.t.int_outputs) v.push_back(eval_postfix(post, m.h_slots.data() + m.slot_base[i]));
+    m.ints[i] = std::move(v);
+  }
+}
+
+const std::vector<int64_t>& BatchRunner::ints(int64_t i) const { return impl_->ints.at(i); }
+
+int64_t BatchRunner::op_count(int64_t i) const {
+  return impl_->progs.at(impl_->inst.at(i).program).t.op_count;
 }
 
 }  // namespace bsz

@@ -22,8 +22,44 @@ class FusedBackend {
   void run(std::vector<Node>& nodes, const Segment& seg, int64_t N, int64_t nw,
            unsigned long long* d_slots, double* compile_ms);
 
+  void set_schedule(const Schedule& s);
+
   int64_t fallbacks = 0;   // parts re-run with the plain kernels (speculation unproven)
   int64_t launches = 0;    // fused kernels launched
+
+  struct Impl;
+
+ private:
+  std::unique_ptr<Impl> impl_;
+};
+
+// ---------------------------------------------------------------------------
+// Batches: many independent instances (stream sets of different lengths) of
+// several straight-line programs, executed by ONE persistent kernel that
+// holds every program's DAG as a device function and pulls (instance, word
+// range) work items from an atomic counter.  The launch (with the resets of
+// its counters) is captured once in a CUDA graph and replayed.
+
+struct BatchInstance {
+  int program = 0;
+  int64_t bitlength = 0;
+  std::vector<const uint64_t*> inputs;   // device pointers, one per scalar input
+  std::vector<uint64_t*> outputs;        // device pointers, one per scalar output (null: skip)
+};
+
+class BatchRunner {
+ public:
+  BatchRunner(Device& dev, const std::vector<const Program*>& progs,
+              std::vector<BatchInstance> instances, const Schedule& sched);
+  ~BatchRunner();
+  void launch();   // asynchronous on the device's stream
+  void finish();   // waits; re-runs per-op if speculation was unproven; reads popcounts
+  const std::vector<int64_t>& ints(int64_t instance) const;
+  int64_t op_count(int64_t instance) const;
+  int64_t n_items() const;
+  double compile_ms = 0.0;
+  int64_t fallbacks = 0;
+  int64_t launches = 0;
 
   struct Impl;
 

@@ -1,0 +1,436 @@
+"""Schedule autotuner and learned cost model for the fused backend.
+
+The fused backend's generated kernels take a schedule (``bsz_schedule`` in
+include/bsz.h): CTA size in warps, the launch-bounds minimum of resident
+CTAs per SM (which caps registers per thread), an occupancy cap, the minimum
+run of 32-word steps a warp owns, software prefetch of the next step's
+loads, and whether ripple adds end a kernel.  The best setting depends on
+the DAG (op mix, shift distances, carry chains, live temporaries) and on the
+stream length, so it is searched, not fixed:
+
+* :data:`CANDIDATES` -- the search space.
+* :func:`measure` -- device time of one (program, length, schedule): the sum
+  of the executor's per-kernel CUDA events over one execution (fused
+  kernels plus any exact re-runs), median over repetitions.
+* :class:`Autotuner` -- exhaustive search, cached in a JSON file keyed by
+  the program text and the length.
+* :class:`CostModel` -- an MLP over DAG features (``bsz_program_features``),
+  log2 length and the schedule encoding, predicting log(ms).  Its training
+  and inference run on the GPU through libbsz's hand-written kernels
+  (``bsz_mlp_*``: tiled FP32 GEMMs with fused bias/ReLU, MSE, column sums,
+  Adam).  :meth:`CostModel.choose` picks a schedule with no measurement,
+  or measures only the ``top_k`` best predictions.
+
+The model is fitted on a random sample of the (program, length, schedule)
+timings of training programs and judged on held-out programs by pick regret:
+time of the picked schedule / time of the exhaustive best - 1.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import itertools
+import json
+import math
+import os
+
+import numpy as np
+
+from . import _lib
+from . import DEFAULT_SCHEDULE, MODE_FUSED, BszError
+
+# ------------------------------------------------------------ search space --
+
+# Knobs that change the generated code (one NVRTC compile each) and knobs
+# that only change the launch.
+CODEGEN_AXES = {"warps": (4, 8), "min_blocks": (2, 4), "prefetch": (0, 1), "cut_adds": (0, 1)}
+LAUNCH_AXES = {"ctas_per_sm": (0, 2)}
+
+
+def candidate_space(codegen=None, launch=None) -> list[dict]:
+    """Cartesian product of the axes, each a full schedule dict."""
+    codegen = codegen or CODEGEN_AXES
+    launch = launch or LAUNCH_AXES
+    keys = list(codegen) + list(launch)
+    out = []
+    for vals in itertools.product(*[codegen[k] for k in codegen], *[launch[k] for k in launch]):
+        s = dict(DEFAULT_SCHEDULE)
+        s.update(dict(zip(keys, vals)))
+        out.append(s)
+    return out
+
+
+CANDIDATES = candidate_space()
+
+
+def schedule_key(s: dict) -> tuple:
+    return tuple(int(s[k]) for k, _ in _lib.Schedule._fields_)
+
+
+def encode_schedule(s: dict) -> list[float]:
+    """Schedule features (7): log2 warps, log2 min_blocks, occupancy cap
+    (0 = none), log2 range_steps, prefetch, cut_adds, log2 threads x
+    min_blocks (the register cap's denominator)."""
+    return [math.log2(s["warps"]), math.log2(max(1, s["min_blocks"])),
+            math.log2(1 + s["ctas_per_sm"]), math.log2(max(1, s["range_steps"])),
+            float(s["prefetch"]), float(s["cut_adds"]),
+            math.log2(32 * s["warps"] * max(1, s["min_blocks"]))]
+
+
+N_SCHEDULE_FEATURES = 7
+
+
+def program_features(prog) -> list[float]:
+    """DAG features of a compiled :class:`Program` (``bsz_program_features``)."""
+    lib = prog.ctx.lib
+    buf = (ctypes.c_float * 64)()
+    n = lib.bsz_program_features(prog.ctx.h, prog.h, buf, 64)
+    if n < 0:
+        raise BszError(_lib.last_error())
+    return list(buf[:n])
+
+
+def feature_row(pfeat: list[float], nbits: int, sched: dict) -> list[float]:
+    return list(pfeat) + [math.log2(max(2, nbits))] + encode_schedule(sched)
+
+
+# ------------------------------------------------------------- measurement --
+
+
+def measure(ctx, prog, nbits: int, inputs: dict, sched: dict, reps: int = 3, warm: int = 1) -> float:
+    """Median device ms of one fused execution under ``sched``.
+
+    ``inputs`` maps input names to device buffers as ``(ptr, n_words)`` (they
+    are bound in place).  The first ``warm`` executions compile the kernels
+    and are not timed."""
+    times = []
+    for i in range(warm + reps):
+        r = prog.run(nbits, MODE_FUSED)
+        r.set_schedule(sched)
+        for k, (ptr, nw) in inputs.items():
+            r.bind(k, ("borrow", ptr, nw))
+        ctx.profile(True)
+        r.execute()
+        rep = ctx.profile_report()
+        ctx.profile(False)
+        del r
+        if i >= warm:
+            times.append(sum(v["ms"] for v in rep.values()))
+    return float(np.median(times))
+
+
+def regret(times: dict, pick) -> float:
+    """Time of the picked schedule over the best in ``times`` (schedule key ->
+    ms), minus one."""
+    best = min(times.values())
+    return times[schedule_key(pick) if isinstance(pick, dict) else pick] / best - 1.0
+
+
+class Autotuner:
+    """Exhaustive search over ``candidates``, cached per (program, length).
+
+    The cache is a JSON file mapping sha1(program text) + ':' + length to the
+    best schedule and every timing."""
+
+    def __init__(self, ctx, candidates=None, cache_path: str | None = None, reps: int = 3):
+        self.ctx = ctx
+        self.candidates = candidates or CANDIDATES
+        self.cache_path = cache_path
+        self.reps = reps
+        self.cache = {}
+        if cache_path and os.path.exists(cache_path):
+            with open(cache_path) as f:
+                self.cache = json.load(f)
+
+    @staticmethod
+    def key(source: str, nbits: int) -> str:
+        return hashlib.sha1(source.encode()).hexdigest() + ":" + str(int(nbits))
+
+    def sweep(self, prog, source: str, nbits: int, inputs: dict) -> dict:
+        """Times every candidate; returns {schedule key: ms}."""
+        k = self.key(source, nbits)
+        if k in self.cache:
+            return {tuple(json.loads(t)): ms for t, ms in self.cache[k]["times"].items()}
+        times = {}
+        for s in self.candidates:
+            times[schedule_key(s)] = measure(self.ctx, prog, nbits, inputs, s, reps=self.reps)
+        best = min(times, key=times.get)
+        self.cache[k] = {"best": list(best), "times": {json.dumps(list(t)): ms for t, ms in times.items()}}
+        if self.cache_path:
+            with open(self.cache_path, "w") as f:
+                json.dump(self.cache, f)
+        return times
+
+    def best(self, prog, source: str, nbits: int, inputs: dict) -> dict:
+        times = self.sweep(prog, source, nbits, inputs)
+        bk = min(times, key=times.get)
+        return dict(zip([k for k, _ in _lib.Schedule._fields_], bk))
+
+
+# -------------------------------------------------------------- cost model --
+
+
+class CostModel:
+    """MLP cost model (in -> hidden x layers -> 1, ReLU, FP32) on libbsz's
+    CUDA kernels.  Inputs are standardised with the training set's mean and
+    standard deviation; the target is standardised log(ms)."""
+
+    def __init__(self, ctx, in_dim: int, hidden: int = 256, layers: int = 3, seed: int = 1):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.in_dim = in_dim
+        self.h = self.lib.bsz_mlp_create(ctx.h, in_dim, hidden, layers, seed)
+        if not self.h:
+            raise BszError(_lib.last_error())
+        self.mu = np.zeros(in_dim, np.float32)
+        self.sd = np.ones(in_dim, np.float32)
+        self.y_mu = 0.0
+        self.y_sd = 1.0
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.lib.bsz_mlp_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    # raw access (standardised units), used by the gradient checks
+    @property
+    def n_params(self) -> int:
+        return int(self.lib.bsz_mlp_num_params(self.h))
+
+    def params(self) -> np.ndarray:
+        p = np.empty(self.n_params, np.float32)
+        _lib.check(self.lib.bsz_mlp_params(self.h, p.ctypes.data, 1))
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.n_params
+        _lib.check(self.lib.bsz_mlp_params(self.h, p.ctypes.data, 0))
+
+    def raw_predict(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        out = np.empty(x.shape[0], np.float32)
+        _lib.check(self.lib.bsz_mlp_predict(self.h, x.ctypes.data, x.shape[0], out.ctypes.data))
+        return out
+
+    def raw_gradients(self, x: np.ndarray, y: np.ndarray) -> tuple[float, np.ndarray]:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        g = np.empty(self.n_params, np.float32)
+        loss = ctypes.c_float()
+        _lib.check(self.lib.bsz_mlp_gradients(self.h, x.ctypes.data, y.ctypes.data, x.shape[0],
+                                               g.ctypes.data, ctypes.byref(loss)))
+        return float(loss.value), g
+
+    def raw_train_step(self, x: np.ndarray, y: np.ndarray, lr: float) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        loss = ctypes.c_float()
+        _lib.check(self.lib.bsz_mlp_train_step(self.h, x.ctypes.data, y.ctypes.data, x.shape[0],
+                                                ctypes.c_float(lr), ctypes.byref(loss)))
+        return float(loss.value)
+
+    # standardised training and prediction
+    def fit(self, X, ms, steps: int = 1500, batch: int = 256, lr: float = 1e-3, seed: int = 0) -> list:
+        """Fits log(ms); returns the loss of every step."""
+        X = np.asarray(X, np.float32)
+        y = np.log(np.asarray(ms, np.float64))
+        self.mu = X.mean(0)
+        self.sd = np.maximum(X.std(0), 1e-3).astype(np.float32)
+        self.y_mu = float(y.mean())
+        self.y_sd = float(max(y.std(), 1e-3))
+        Xs = (X - self.mu) / self.sd
+        ys = ((y - self.y_mu) / self.y_sd).astype(np.float32)
+        rng = np.random.default_rng(seed)
+        losses = []
+        n = Xs.shape[0]
+        for t in range(steps):
+            idx = rng.integers(0, n, size=min(batch, n))
+            # cosine decay to 5% of the initial rate
+            rate = lr * (0.05 + 0.95 * 0.5 * (1 + math.cos(math.pi * t / max(1, steps))))
+            losses.append(self.raw_train_step(Xs[idx], ys[idx], rate))
+        return losses
+
+    def predict_ms(self, X) -> np.ndarray:
+        X = (np.asarray(X, np.float32) - self.mu) / self.sd
+        return np.exp(self.raw_predict(X).astype(np.float64) * self.y_sd + self.y_mu)
+
+    def rank(self, pfeat: list[float], nbits: int, candidates=None) -> list[dict]:
+        """Candidates sorted by predicted time (fastest first)."""
+        candidates = candidates or CANDIDATES
+        pred = self.predict_ms([feature_row(pfeat, nbits, s) for s in candidates])
+        return [candidates[i] for i in np.argsort(pred, kind="stable")]
+
+    def choose(self, prog, nbits: int, candidates=None, top_k: int = 1, inputs: dict | None = None,
+               reps: int = 3) -> dict:
+        """The predicted-fastest schedule; with ``top_k`` > 1 (and device
+        ``inputs``) the fastest measured of the ``top_k`` best predictions."""
+        ranked = self.rank(program_features(prog), nbits, candidates)
+        if top_k <= 1 or inputs is None:
+            return ranked[0]
+        timed = [(measure(self.ctx, prog, nbits, inputs, s, reps=reps), i) for i, s in enumerate(ranked[:top_k])]
+        return ranked[min(timed)[1]]
+
+    def save(self, path: str):
+        np.savez(path, params=self.params(), mu=self.mu, sd=self.sd, y=np.array([self.y_mu, self.y_sd]),
+                 in_dim=np.array([self.in_dim]))
+
+    def load(self, path: str):
+        z = np.load(path)
+        assert int(z["in_dim"][0]) == self.in_dim
+        self.set_params(z["params"])
+        self.mu, self.sd = z["mu"], z["sd"]
+        self.y_mu, self.y_sd = float(z["y"][0]), float(z["y"][1])
+
+
+# ------------------------------------------------------------------- study --
+
+
+def tuning_suite(n_train: int = 24, n_test: int = 8, seed: int = 20261210, max_ops: int = 3000):
+    """Seeded training and held-out program sources.
+
+    Each DAG draws its op mix from Dirichlet(1) over five classes (AND/OR/
+    XOR, shift left, ADD, shift right, NOT), its size log-uniformly from 50
+    to ``max_ops`` generator ops, an operand window from {all, 6, 24, 96}
+    and a maximum shift distance from {1, 7, 70}.  The held-out set ends
+    with the 300- and 2,000-op regex-shaped DAGs."""
+    from .workloads import regex_dag_src, shaped_dag_src
+
+    rng = np.random.default_rng(seed)
+
+    def draw(k):
+        p = rng.dirichlet(np.ones(5))
+        n_ops = int(round(math.exp(rng.uniform(math.log(50), math.log(max_ops)))))
+        return shaped_dag_src(n_ops=n_ops, seed=seed + k, window=int(rng.choice([0, 6, 24, 96])),
+                              p_bit=float(p[0]), p_shl=float(p[1]), p_add=float(p[2]), p_shr=float(p[3]),
+                              max_shift=int(rng.choice([1, 7, 70])))
+
+    train = [draw(k) for k in range(n_train)]
+    test = [draw(1000 + k) for k in range(max(0, n_test - 2))]
+    test += [regex_dag_src(n_ops=300, seed=seed + 7), regex_dag_src(n_ops=2000)][: max(0, n_test)]
+    return train, test
+
+
+def _device_inputs(nbits: int, n_inputs: int, seed: int):
+    import torch
+
+    nw = (nbits + 63) // 64
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    bufs = [torch.randint(-2**63, 2**63 - 1, (nw,), dtype=torch.int64, device="cuda", generator=g)
+            for _ in range(n_inputs)]
+    if nbits % 64:
+        mask = (1 << (nbits % 64)) - 1
+        for b in bufs:
+            b[-1:].bitwise_and_(mask if mask < 2**63 else mask - 2**64)
+    torch.cuda.synchronize()
+    return bufs, {f"b{i}": (b.data_ptr(), nw) for i, b in enumerate(bufs)}
+
+
+def study(ctx, train_srcs, test_srcs, sizes=(1 << 23, 1 << 25, 1 << 27), candidates=None,
+          sample_frac: float = 0.25, reps: int = 3, steps: int = 1500, seed: int = 0, log=None) -> dict:
+    """Collects timings (a ``sample_frac`` sample of the candidates for each
+    training (program, length); every candidate for held-out ones), fits a
+    :class:`CostModel` and reports pick regret on the held-out programs for
+    the model's top-1 and top-4 picks and for the default schedule."""
+    import time as _time
+
+    candidates = candidates or CANDIDATES
+    rng = np.random.default_rng(seed)
+    t0 = _time.time()
+    X, y = [], []
+    n_timed = 0
+    bufs_by_size = {n: _device_inputs(n, 8, seed + n % 997) for n in sizes}
+    progs = {}
+
+    def prog_of(src):
+        if src not in progs:
+            progs[src] = (ctx.compile(src), None)
+            progs[src] = (progs[src][0], program_features(progs[src][0]))
+        return progs[src]
+
+    for i, src in enumerate(train_srcs):
+        prog, pf = prog_of(src)
+        for n in sizes:
+            k = max(1, int(round(sample_frac * len(candidates))))
+            for j in rng.choice(len(candidates), size=k, replace=False):
+                ms = measure(ctx, prog, n, bufs_by_size[n][1], candidates[j], reps=reps)
+                X.append(feature_row(pf, n, candidates[j]))
+                y.append(ms)
+                n_timed += 1
+        if log:
+            log(f"train {i + 1}/{len(train_srcs)} timed={n_timed} t={_time.time() - t0:.0f}s")
+    t_collect = _time.time() - t0
+    model = CostModel(ctx, len(X[0]), seed=seed + 1)
+    t1 = _time.time()
+    losses = model.fit(X, y, steps=steps, seed=seed)
+    t_fit = _time.time() - t1
+
+    default_key = schedule_key(DEFAULT_SCHEDULE)
+    rows = []
+    for i, src in enumerate(test_srcs):
+        prog, pf = prog_of(src)
+        for n in sizes:
+            times = {schedule_key(s): measure(ctx, prog, n, bufs_by_size[n][1], s, reps=reps)
+                     for s in candidates}
+            if default_key not in times:
+                times[default_key] = measure(ctx, prog, n, bufs_by_size[n][1], DEFAULT_SCHEDULE, reps=reps)
+            ranked = model.rank(pf, n, candidates)
+            top4 = min(times[schedule_key(s)] for s in ranked[:4])
+            best = min(times.values())
+            rows.append({"program": i, "ops": int(round(2 ** pf[0] - 1)), "bits": n, "best_ms": best,
+                         "best": list(min(times, key=times.get)),
+                         "regret_top1": times[schedule_key(ranked[0])] / best - 1,
+                         "regret_top4": top4 / best - 1,
+                         "regret_default": times[default_key] / best - 1})
+        if log:
+            log(f"test {i + 1}/{len(test_srcs)} t={_time.time() - t0:.0f}s")
+
+    def stats(key):
+        v = np.array([r[key] for r in rows])
+        return {"mean": float(v.mean()), "median": float(np.median(v)), "max": float(v.max())}
+
+    return {"model": model, "rows": rows, "n_candidates": len(candidates), "n_train_programs": len(train_srcs),
+            "n_test_programs": len(test_srcs), "sizes": list(sizes), "sample_frac": sample_frac,
+            "n_train_timings": n_timed, "loss_first": float(np.mean(losses[:20])),
+            "loss_last": float(np.mean(losses[-20:])), "collect_s": t_collect, "fit_s": t_fit,
+            "regret_top1": stats("regret_top1"), "regret_top4": stats("regret_top4"),
+            "regret_default": stats("regret_default"),
+            "exhaustive_timings_per_case": len(candidates)}
+
+
+def main(argv=None):
+    """python -m bitstreamzoo_b200.tuner [--out model.npz] [--json report.json]
+    runs :func:`study` on the default suite and saves the fitted model."""
+    import argparse
+
+    from . import Context
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--json", default=None)
+    ap.add_argument("--train", type=int, default=24)
+    ap.add_argument("--test", type=int, default=8)
+    ap.add_argument("--sample-frac", type=float, default=0.25)
+    ap.add_argument("--steps", type=int, default=1500)
+    a = ap.parse_args(argv)
+    ctx = Context(0)
+    train, test = tuning_suite(a.train, a.test)
+    rep = study(ctx, train, test, sample_frac=a.sample_frac, steps=a.steps,
+                log=lambda m: print(m, flush=True))
+    model = rep.pop("model")
+    if a.out:
+        model.save(a.out)
+    summary = {k: v for k, v in rep.items() if k != "rows"}
+    print(json.dumps(summary))
+    if a.json:
+        with open(a.json, "w") as f:
+            json.dump(rep, f, indent=1)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -221,6 +221,62 @@ def regex_dag_src(n_ops: int = 2000, seed: int = 20261206, n_outputs: int = 4) -
     return "\n".join(lines + body) + "\n"
 
 
+def batched_plan(n_instances: int = 4096, n_dags: int = 16, lo_log2: int = 12, hi_log2: int = 26,
+                 ops: int = 300, seed: int = 20261207):
+    """Batched uneven instances: ``n_dags`` seeded regex-shaped DAGs of ``ops``
+    generator ops (the regex_dag mix, 8 basis inputs, 4 outputs + popcounts)
+    and ``n_instances`` stream lengths drawn log-uniformly from
+    [2^lo_log2, 2^hi_log2] bits; instance i runs DAG i mod n_dags.
+    Returns (list of program sources, list of (dag, bits))."""
+    rng = _rng(seed)
+    srcs = [regex_dag_src(n_ops=ops, seed=seed + 1 + k) for k in range(n_dags)]
+    logs = rng.uniform(lo_log2, hi_log2, size=n_instances)
+    bits = np.maximum(1, np.floor(np.exp2(logs))).astype(np.int64)
+    return srcs, [(i % n_dags, int(bits[i])) for i in range(n_instances)]
+
+
+def shaped_dag_src(n_ops: int, seed: int, window: int = 0, p_bit: float = 0.55, p_shl: float = 0.2,
+                   p_add: float = 0.1, p_shr: float = 0.0, max_shift: int = 1, n_inputs: int = 8,
+                   n_outputs: int = 4) -> str:
+    """Seeded DAG with a chosen shape, for schedule tuning.
+
+    Operands come from the last ``window`` values (0 = all values so far, as
+    in :func:`regex_dag_src`): a small window gives deep chains with few live
+    temporaries, a large one wide DAGs.  Op classes are drawn with the given
+    probabilities (the rest are NOTs); shift distances are uniform in
+    [1, max_shift].  Outputs are the last ``n_outputs`` values and their
+    popcounts."""
+    rng = _rng(seed)
+    vals = [f"b{i}" for i in range(n_inputs)]
+    lines = [f"input stream b{i}" for i in range(n_inputs)]
+    lines += [f"output stream o{j}" for j in range(n_outputs)]
+    lines += [f"output int p{j}" for j in range(n_outputs)]
+    body = []
+    for i in range(n_ops):
+        lo = 0 if window <= 0 else max(0, len(vals) - window)
+
+        def pick():
+            return vals[int(rng.integers(lo, len(vals)))]
+
+        d = f"v{i}"
+        u = float(rng.random())
+        if u < p_bit:
+            body.append(f"stream {d} = {pick()} {'&|^'[int(rng.integers(0, 3))]} {pick()}")
+        elif u < p_bit + p_shl:
+            body.append(f"stream {d} = {pick()} << {int(rng.integers(1, max_shift + 1))}")
+        elif u < p_bit + p_shl + p_add:
+            body.append(f"stream {d} = {pick()} + {pick()}")
+        elif u < p_bit + p_shl + p_add + p_shr:
+            body.append(f"stream {d} = {pick()} >> {int(rng.integers(1, max_shift + 1))}")
+        else:
+            body.append(f"stream {d} = ~{pick()}")
+        vals.append(d)
+    for j in range(n_outputs):
+        body.append(f"o{j} = {vals[-1 - j]}")
+        body.append(f"p{j} = popcount(o{j})")
+    return "\n".join(lines + body) + "\n"
+
+
 def regex_dag_inputs(nbits: int = 1 << 29, seed: int = 20261205) -> dict:
     streams = basis_bits(regex_bytes(nbits, seed))
     return {f"b{i}": s for i, s in enumerate(streams)}

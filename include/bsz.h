@@ -55,6 +55,18 @@ typedef struct bsz_stats {
   int64_t n_fused_fallbacks; /* segment parts re-run per-op because speculation was unproven */
 } bsz_stats;
 
+/* Schedule of the generated segment kernels (fused form).  The autotuner and
+ * the learned cost model choose among these; zero-initialised fields of a
+ * default schedule are {4, 64, 0, 4, 1, 0}. */
+typedef struct bsz_schedule {
+  int32_t warps;        /* warps per CTA (1..16) */
+  int32_t range_steps;  /* minimum 32-word steps owned by one warp (words per tile / 32) */
+  int32_t ctas_per_sm;  /* resident CTAs per SM, 0 = as many as occupancy allows */
+  int32_t min_blocks;   /* launch-bounds minimum blocks per SM (caps registers) */
+  int32_t prefetch;     /* 1: load the next 32-word step before computing this one */
+  int32_t cut_adds;     /* 1: materialize every addition (one kernel per addition level) */
+} bsz_schedule;
+
 /* ---- library ---------------------------------------------------------- */
 const char* bsz_version(void);
 const char* bsz_last_error(void);
@@ -84,6 +96,8 @@ int64_t bsz_static_ops(bsz_program* prog, const char* const* param_names,
 bsz_run* bsz_run_create(bsz_program* prog, int64_t bitlength, int mode);
 void bsz_run_free(bsz_run* run);
 int bsz_set_param(bsz_run* run, const char* name, int64_t value);
+/* Sets the fused-kernel schedule for this run (before bsz_execute). */
+int bsz_run_set_schedule(bsz_run* run, const bsz_schedule* schedule);
 /* Binds an input stream.  index < 0: scalar input; index >= 0: element of an
  * input array.  `words` holds n_words words on the host (on_device = 0, the
  * copy is made on the context's stream) or on the device (on_device = 1, the
@@ -111,6 +125,56 @@ int bsz_get_int(bsz_run* run, const char* name, int64_t* value);
 /* Indices present in an array output; returns the count (<= cap written),
  * or -1 if the array does not exist. */
 int64_t bsz_array_indices(bsz_run* run, const char* name, int64_t* indices, int64_t cap);
+
+/* ---- batches: many independent instances in one launch ------------------
+ * Several straight-line programs (no if/while on streams, no input/output
+ * arrays, no right shift of a temporary) run over many instances of
+ * different stream lengths by ONE persistent kernel that holds every
+ * program's DAG and pulls (instance, word range) items from a work queue.
+ * bsz_batch_create traces and compiles once and captures the launch in a
+ * CUDA graph; bsz_batch_launch replays it (asynchronous); bsz_batch_finish
+ * waits and reads every instance's popcount results.  No reference
+ * counterpart: the reference runs one process per case
+ * (benchmark/base.py:228-254). */
+typedef struct bsz_instance {
+  int32_t program;                 /* index into the programs array */
+  int64_t bitlength;               /* this instance's stream length in bits */
+  const uint64_t* const* inputs;   /* device pointers, one per declared scalar input */
+  uint64_t* const* outputs;        /* device pointers, one per declared output stream (NULL: skip) */
+} bsz_instance;
+typedef struct bsz_batch bsz_batch;
+bsz_batch* bsz_batch_create(bsz_ctx* ctx, bsz_program* const* programs, int n_programs,
+                            const bsz_instance* instances, int64_t n_instances,
+                            const bsz_schedule* schedule);
+int bsz_batch_launch(bsz_batch* batch);
+int bsz_batch_finish(bsz_batch* batch, bsz_stats* stats);
+/* Output ints of one instance (declaration order); returns how many. */
+int bsz_batch_ints(bsz_batch* batch, int64_t instance, int64_t* values, int capacity);
+int64_t bsz_batch_items(bsz_batch* batch);
+void bsz_batch_free(bsz_batch* batch);
+
+/* ---- learned schedule cost model ------------------------------------------
+ * A small FP32 MLP (in_dim -> hidden x layers (ReLU) -> 1) trained with Adam
+ * on MSE by hand-written CUDA kernels on the context's stream.  x is n rows
+ * of in_dim floats (row-major, host), y / out n floats (host).  No reference
+ * counterpart. */
+/* DAG features of a straight-line program for the cost model (traced and
+ * simplified as the fused form sees it): writes up to `capacity` floats,
+ * returns the number of features (BSZ_NUM_FEATURES) or -1 on error. */
+#define BSZ_NUM_FEATURES 14
+int bsz_program_features(bsz_ctx* ctx, bsz_program* prog, float* out, int capacity);
+typedef struct bsz_mlp bsz_mlp;
+bsz_mlp* bsz_mlp_create(bsz_ctx* ctx, int in_dim, int hidden, int layers, uint64_t seed);
+int64_t bsz_mlp_num_params(bsz_mlp* mlp);
+/* One Adam step; *loss = the batch loss before the step. */
+int bsz_mlp_train_step(bsz_mlp* mlp, const float* x, const float* y, int n, float lr, float* loss);
+int bsz_mlp_predict(bsz_mlp* mlp, const float* x, int n, float* out);
+/* Loss and its gradient w.r.t. the flat parameters (no update). */
+int bsz_mlp_gradients(bsz_mlp* mlp, const float* x, const float* y, int n, float* grad, float* loss);
+/* Flat parameters W1 b1 W2 b2 ... Wout bout (each W row-major [fan_in, fan_out]);
+ * get != 0 copies them out, get == 0 loads them (and resets Adam state). */
+int bsz_mlp_params(bsz_mlp* mlp, float* params, int get);
+void bsz_mlp_free(bsz_mlp* mlp);
 
 /* ---- whole-case driver (replaces run_case<64>, main.cu:23-207) ----------
  * Runs `source` on every case of a .bsdata file (or, if bsdata_path is NULL,
@@ -144,6 +208,14 @@ int bsz_op_shr(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, uint64_t k, uint6
                int tail);
 int bsz_op_popcount(bsz_ctx* ctx, const uint64_t* a, uint64_t n_words, uint64_t* result);
 int bsz_op_is_nonzero(bsz_ctx* ctx, const uint64_t* a, uint64_t n_words, int* result);
+
+/* Byte -> basis-bit transposition on the device (replaces
+ * payload_to_basis_bits / payload_to_basis_bits_fast,
+ * benchmark/apps/regex/src/run.py:164-187): bit j of basis stream i = bit i
+ * of bytes[j].  `bytes` (n_bytes) and the eight `basis[i]` (ceil(n_bytes/64)
+ * words each) are device pointers; bits at and above n_bytes are zero.
+ * Asynchronous on the context's stream. */
+int bsz_s2p(bsz_ctx* ctx, const uint8_t* bytes, int64_t n_bytes, uint64_t* const* basis);
 
 /* Stream addition that allocates no device memory (no counterpart in the
  * reference).  For callers that cannot allocate GPU memory when they call:

@@ -21,7 +21,7 @@ def header_symbols():
     with open(os.path.join(ROOT, "include", "bsz.h")) as f:
         text = f.read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(bsz_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(bsz_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol():

@@ -155,3 +155,15 @@ def test_c_oracle_random_straight_line_vs_pyoracle():
         mask = (1 << nbits) - 1
         for k in ("out0", "out1"):
             assert cwords.words_to_int(outs[k]) & mask == ref[k] & mask
+
+
+def test_basis_restatements_agree():
+    from oracle import basis
+    rng = np.random.default_rng(17)
+    for n in (0, 1, 7, 63, 64, 65, 200, 1000):
+        payload = rng.integers(0, 256, n, dtype=np.uint8).tobytes()
+        ints = basis.basis_ints(payload)
+        words = basis.basis_words(payload)
+        for i in range(8):
+            assert cwords.words_to_int(words[i]) == ints[i]
+            assert words[i].size == (n + 63) // 64
