@@ -104,6 +104,25 @@ class Workload:
         return table.get(kname, float("nan"))
 
 
+def alu_roofline(prog, nbits: int, launch_ms: float, clocks) -> dict:
+    """Integer-pipe roofline of a fused launch.  Algorithmic INT32 lane
+    operations per 64-bit word of the post-DCE DAG: 2 per AND/OR/XOR/NOT/
+    ANDNOT, 4 per shift (two funnel shifts and the neighbour word), 6 per ADD
+    (64-bit add, carry-generate compare, carry-in add).  Peak: 148 SMs x 128
+    INT32 lanes x the median SM clock seen while timing."""
+    from bitstreamzoo_b200 import tuner
+    f = tuner.program_features(prog)
+    n_ops = round(2 ** f[0] - 1)
+    per_word = n_ops * (2 * (f[1] + f[2]) + 4 * (f[3] + f[4] + f[6]) + 6 * f[5])
+    words = (nbits + 63) // 64
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    peak = 148 * 128 * mhz * 1e6 / 1e12
+    achieved = per_word * words / (launch_ms * 1e-3) / 1e12
+    return {"bound": "int32", "dag_ops": n_ops, "int32_ops_per_word": per_word, "achieved": achieved,
+            "peak": peak, "unit": "Tops/s", "frac": achieved / peak,
+            "peak_source": "nominal 148 SMs x 128 lanes x measured median SM clock"}
+
+
 DEFAULT_BITS = {"long_streams": 1 << 32, "regex_dag": 1 << 29, "matchstar": 1 << 24}
 DEFAULT_CPU_SAMPLE = {"long_streams": 1 << 28, "regex_dag": 1 << 26, "matchstar": 1 << 24}
 
@@ -415,6 +434,8 @@ def run_ours(args, rank, world, local):
                     "traffic": traffic, "bytes_per_launch": bytes_launch,
                     "launch_ms": per_launch_ms,
                     "kernel_share": kv["ms"] / max(1e-9, sum(x["ms"] for x in prof.values()))}
+            if kname.startswith("fused"):
+                roof["alu"] = alu_roofline(prog, nbits, per_launch_ms, main.get("clocks"))
         line = {
             "metric": metric_name(args.workload),
             "value": main.get("value"), "unit": "GB/s", "n_gpus": world, "steps": args.steps,

@@ -27,11 +27,15 @@ from ._lib import BszError, Stats
 
 MODE_PLAIN = 0
 MODE_FUSED = 1
+MODE_AUTO = 2
+MODE_VM = 3
+MODES = {"plain": MODE_PLAIN, "fused": MODE_FUSED, "auto": MODE_AUTO, "vm": MODE_VM}
 
 DEFAULT_SCHEDULE = {"warps": 4, "range_steps": 64, "ctas_per_sm": 0, "min_blocks": 4,
                     "prefetch": 1, "cut_adds": 0}
 
 __all__ = ["Context", "Program", "Run", "B200Backend", "BszError", "MODE_PLAIN", "MODE_FUSED",
+           "MODE_AUTO", "MODE_VM",
            "int_to_words", "words_to_int", "bsim_cuda_path"]
 
 
@@ -116,8 +120,11 @@ class Context:
 
     def run_case_json(self, source: str, bsdata_path: str | None = None,
                       json_input: dict | None = None, warmup: bool = False,
-                      fused: bool = True):
-        flags = (1 if warmup else 0) | (2 if fused else 0)
+                      mode="auto"):
+        """bsim_cuda JSON for every case; ``mode`` is a name of ``MODES`` or
+        a ``MODE_*`` value."""
+        m = MODES[mode] if isinstance(mode, str) else int(mode)
+        flags = (1 if warmup else 0) | (m << 1)
         js = self.lib.bsz_run_case_json(
             self.h, source.encode(), bsdata_path.encode() if bsdata_path else None,
             json.dumps(json_input).encode() if json_input is not None else None, flags)
@@ -337,15 +344,15 @@ class B200Backend:
     ``ProgramInfo`` (anything with ``source_path``) or DSL source text.
     """
 
-    def __init__(self, device: int = 0, fused: bool = True, ctx: Context | None = None):
+    def __init__(self, device: int = 0, mode="auto", ctx: Context | None = None):
         self.ctx = ctx or Context(device)
-        self.fused = fused
+        self.mode = mode
 
     def run(self, prog, inputs, params=None, input_arrays=None, bitlength=0,
             iterations=1, feedback=None, bsdata_path=None):
         src = _source_of(prog)
         if bsdata_path:
-            out = self.ctx.run_case_json(src, bsdata_path=bsdata_path, fused=self.fused)
+            out = self.ctx.run_case_json(src, bsdata_path=bsdata_path, mode=self.mode)
         else:
             payload = {"inputs": {k: hex(v) for k, v in inputs.items()},
                        "params": params or {}, "n_vectors": bitlength}
@@ -357,14 +364,14 @@ class B200Backend:
                 payload["iterations"] = iterations
             if feedback:
                 payload["feedback"] = feedback
-            out = self.ctx.run_case_json(src, json_input=payload, fused=self.fused)
+            out = self.ctx.run_case_json(src, json_input=payload, mode=self.mode)
         return _parse_outputs(out["outputs"]), out["op_count"], out.get("exec_ms", 0.0)
 
     def run_batch(self, prog, bsdata_paths):
         src = _source_of(prog)
         results = []
         for p in bsdata_paths:
-            out = self.ctx.run_case_json(src, bsdata_path=p, fused=self.fused)
+            out = self.ctx.run_case_json(src, bsdata_path=p, mode=self.mode)
             results.extend(out if isinstance(out, list) else [out])
         return results
 

@@ -23,7 +23,7 @@ class Stats(ctypes.Structure):
                 ("n_syncs", ctypes.c_int64), ("peak_bytes", ctypes.c_int64),
                 ("max_live", ctypes.c_int64), ("kernel_ms", ctypes.c_double),
                 ("compile_ms", ctypes.c_double), ("n_fused_launches", ctypes.c_int64),
-                ("n_fused_fallbacks", ctypes.c_int64)]
+                ("n_fused_fallbacks", ctypes.c_int64), ("n_vm_launches", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -87,6 +87,7 @@ SIGNATURES = {
     "bsz_mlp_gradients": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int, c_void_p,
                                          ctypes.POINTER(ctypes.c_float)]),
     "bsz_mlp_params": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int]),
+    "bsz_mlp_set_weight_decay": (ctypes.c_int, [c_void_p, ctypes.c_float]),
     "bsz_mlp_free": (None, [c_void_p]),
     "bsz_run_case_json": (ctypes.c_char_p, [c_void_p, ctypes.c_char_p, ctypes.c_char_p,
                                             ctypes.c_char_p, ctypes.c_int]),

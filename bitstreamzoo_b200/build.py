@@ -33,9 +33,9 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-Wall,-Wno-unus
           "-I", CSRC, "-I", os.path.join(ROOT, "include")]
 
 LIB_SOURCES = ["frontend.cpp", "device.cu", "kernels.cu", "engine.cpp", "fused.cpp", "io.cpp",
-               "capi.cpp", "noalloc.cu", "mlp.cu", "s2p.cu"]
+               "capi.cpp", "noalloc.cu", "mlp.cu", "s2p.cu", "vm.cu"]
 MAIN_SOURCES = ["bsim_main.cpp"]
-HEADERS = ["frontend.h", "device.h", "engine.h", "fused.h", "io.h", "mlp.h", "s2p.h"]
+HEADERS = ["frontend.h", "device.h", "engine.h", "fused.h", "io.h", "mlp.h", "s2p.h", "vm.h"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -8,7 +8,7 @@
 // prints to stderr and exits 1 ("out of memory" is preserved in the message
 // so the harness maps it to MemoryError, benchmark/base.py:219-223).
 //
-// Additional flag: --mode=plain|fused (default: $BSZ_MODE, else fused).
+// Additional flag: --mode=plain|fused|auto|vm (default: $BSZ_MODE, else auto).
 // --word-bits=32 is accepted; results do not depend on the word width, and
 // the executor always computes on 64-bit words.
 #include <chrono>
@@ -25,14 +25,20 @@
 int main(int argc, char** argv) {
   if (argc < 2) {
     std::cerr << "Usage: bsim_cuda program.bs [--trace] [--word-bits=32|64] [--reuse-mem] "
-                 "[--warmup] [--input file.bsdata ...] [--dump-input] [--mode=plain|fused]\n";
+                 "[--warmup] [--input file.bsdata ...] [--dump-input] [--mode=plain|fused|auto|vm]\n";
     return 1;
   }
   std::string bs_path = argv[1];
   bool dump_input = false;
   bsz::DriverOptions opt;
+  auto mode_of = [](const std::string& m) {
+    if (m == "plain") return 0;
+    if (m == "fused") return 1;
+    if (m == "vm") return 3;
+    return 2;
+  };
   const char* env_mode = std::getenv("BSZ_MODE");
-  opt.mode = (env_mode && !std::strcmp(env_mode, "plain")) ? 0 : 1;
+  opt.mode = env_mode ? mode_of(env_mode) : 2;
   int word_bits = 64;
   std::vector<std::string> inputs;
   for (int i = 2; i < argc; ++i) {
@@ -48,7 +54,7 @@ int main(int argc, char** argv) {
     } else if (a == "--dump-input") {
       dump_input = true;
     } else if (a.rfind("--mode=", 0) == 0) {
-      opt.mode = a.substr(7) == "plain" ? 0 : 1;
+      opt.mode = mode_of(a.substr(7));
     }
   }
   if (word_bits != 32 && word_bits != 64) {
@@ -85,6 +91,9 @@ int main(int argc, char** argv) {
     std::string out = cases.size() > 1 ? "[" : "";
     for (size_t ci = 0; ci < cases.size(); ++ci) {
       auto& c = cases[ci];
+      for (auto& kv : c.inputs) kv.second.materialize();
+      for (auto& kv : c.arrays)
+        for (auto& e : kv.second) e.second.materialize();
       if (ci) out += ",";
       out += "{\"bitlength\":" + std::to_string(c.bitlength) + ",\"inputs\":{";
       bool first = true;

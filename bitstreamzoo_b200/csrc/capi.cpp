@@ -76,7 +76,7 @@ int64_t words_of(int64_t bitlength) { return bitlength > 0 ? (bitlength + 63) / 
 bsz::Executor& executor(bsz_run* r) {
   if (!r->ex) {
     bsz::ExecOptions o;
-    o.mode = r->mode == BSZ_MODE_FUSED ? bsz::ExecMode::Fused : bsz::ExecMode::Plain;
+    o.mode = static_cast<bsz::ExecMode>(r->mode);
     r->ex = std::make_unique<bsz::Executor>(*r->prog->ctx->dev, *r->prog->prog, r->bitlength, o);
   }
   return *r->ex;
@@ -173,6 +173,7 @@ bsz_run* bsz_run_create(bsz_program* prog, int64_t bitlength, int mode) {
         auto run = std::make_unique<bsz_run>();
         run->prog = prog;
         run->bitlength = bitlength;
+        if (mode < BSZ_MODE_PLAIN || mode > BSZ_MODE_VM) throw bsz::RuntimeError("bsz_run_create: bad mode");
         run->mode = mode;
         ++prog->refs;
         try {
@@ -289,6 +290,7 @@ int bsz_execute(bsz_run* run, bsz_stats* stats) {
       stats->compile_ms = ex.compile_ms;
       stats->n_fused_launches = ex.fused_launches();
       stats->n_fused_fallbacks = ex.fused_fallbacks();
+      stats->n_vm_launches = ex.vm_launches;
     }
   });
 }
@@ -459,6 +461,13 @@ int bsz_mlp_params(bsz_mlp* m, float* params, int get) {
   });
 }
 
+int bsz_mlp_set_weight_decay(bsz_mlp* m, float weight_decay) {
+  return guard([&] {
+    if (!(weight_decay >= 0.f)) throw bsz::RuntimeError("bsz_mlp_set_weight_decay: negative or NaN");
+    m->net->set_weight_decay(weight_decay);
+  });
+}
+
 void bsz_mlp_free(bsz_mlp* m) {
   if (!m) return;
   bsz_ctx* c = m->ctx;
@@ -570,7 +579,7 @@ const char* bsz_run_case_json(bsz_ctx* ctx, const char* source, const char* bsda
     else cases.push_back(bsz::parse_json_case(json_input ? json_input : "{}"));
     bsz::DriverOptions o;
     o.warmup = flags & 1;
-    o.mode = (flags & 2) ? 1 : 0;
+    o.mode = (flags >> 1) & 3;
     if (cases.size() == 1) {
       g_json = bsz::run_case_json(*ctx->dev, *prog, cases[0], o, parse_ms);
     } else {

@@ -3,6 +3,9 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
+#include <thread>
+#include <vector>
 
 namespace bsz {
 
@@ -31,7 +34,91 @@ Device::~Device() {
   if (d_scan_) cudaFree(d_scan_);
   if (d_err_) cudaFree(d_err_);
   if (d_scratch_) cudaFree(d_scratch_);
+  for (int k = 0; k < 2; ++k) {
+    if (pin_[k]) cudaFreeHost(pin_[k]);
+    if (pin_ev_[k]) cudaEventDestroy(pin_ev_[k]);
+  }
   if (stream_) cudaStreamDestroy(stream_);
+}
+
+namespace {
+
+constexpr size_t kStageBytes = size_t(32) << 20;
+constexpr size_t kDirectBytes = size_t(1) << 20;
+
+// memcpy split across host threads for large chunks.
+void parallel_memcpy(void* dst, const void* src, size_t n) {
+  const size_t kMinPerThread = size_t(4) << 20;
+  unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  size_t nt = std::min<size_t>({static_cast<size_t>(hw), size_t(8), n / kMinPerThread});
+  if (nt <= 1) {
+    std::memcpy(dst, src, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t per = (n + nt - 1) / nt;
+  for (size_t t = 0; t < nt; ++t) {
+    const size_t off = t * per;
+    if (off >= n) break;
+    const size_t len = std::min(per, n - off);
+    th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off, len); });
+  }
+  for (auto& t : th) t.join();
+}
+
+}  // namespace
+
+void Device::ensure_pinned() {
+  if (pin_[0]) return;
+  for (int k = 0; k < 2; ++k) {
+    BSZ_CUDA(cudaHostAlloc(&pin_[k], kStageBytes, cudaHostAllocDefault));
+    BSZ_CUDA(cudaEventCreateWithFlags(&pin_ev_[k], cudaEventDisableTiming));
+    BSZ_CUDA(cudaEventRecord(pin_ev_[k], stream_));
+  }
+}
+
+void Device::h2d(void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return;
+  if (bytes <= kDirectBytes) {
+    BSZ_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_));
+    return;
+  }
+  ensure_pinned();
+  int k = 0;
+  for (size_t off = 0; off < bytes; off += kStageBytes, k ^= 1) {
+    const size_t len = std::min(kStageBytes, bytes - off);
+    BSZ_CUDA(cudaEventSynchronize(pin_ev_[k]));   // its previous DMA is done
+    parallel_memcpy(pin_[k], static_cast<const char*>(src) + off, len);
+    BSZ_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + off, pin_[k], len, cudaMemcpyHostToDevice, stream_));
+    BSZ_CUDA(cudaEventRecord(pin_ev_[k], stream_));
+  }
+}
+
+void Device::d2h(void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return;
+  if (bytes <= kDirectBytes) {
+    BSZ_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream_));
+    BSZ_CUDA(cudaStreamSynchronize(stream_));
+    return;
+  }
+  ensure_pinned();
+  // chunk i DMAs into pin_[i & 1]; the host copies chunk i-1 out meanwhile
+  size_t prev_off = 0, prev_len = 0;
+  int k = 0;
+  for (size_t off = 0; off < bytes; off += kStageBytes, k ^= 1) {
+    const size_t len = std::min(kStageBytes, bytes - off);
+    BSZ_CUDA(cudaEventSynchronize(pin_ev_[k]));
+    BSZ_CUDA(cudaMemcpyAsync(pin_[k], static_cast<const char*>(src) + off, len, cudaMemcpyDeviceToHost, stream_));
+    BSZ_CUDA(cudaEventRecord(pin_ev_[k], stream_));
+    if (prev_len) {
+      BSZ_CUDA(cudaEventSynchronize(pin_ev_[k ^ 1]));
+      parallel_memcpy(static_cast<char*>(dst) + prev_off, pin_[k ^ 1], prev_len);
+    }
+    prev_off = off;
+    prev_len = len;
+  }
+  BSZ_CUDA(cudaEventSynchronize(pin_ev_[k ^ 1]));
+  parallel_memcpy(static_cast<char*>(dst) + prev_off, pin_[k ^ 1], prev_len);
 }
 
 void* Device::raw_alloc(size_t bytes) {

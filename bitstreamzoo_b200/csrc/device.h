@@ -79,6 +79,16 @@ class Device {
   // Untyped device scratch (cached; grows).
   void* scratch(size_t bytes);
 
+  // Copies between pageable host memory and the device through two pinned
+  // staging buffers: chunks are double-buffered (the host memcpy of one
+  // chunk, split across threads, overlaps the DMA of the other), so large
+  // transfers run at link speed instead of the driver's pageable path.
+  // h2d returns once `src` may be reused (the last DMA may still be in
+  // flight on the stream); d2h returns with `dst` filled.  Small copies go
+  // straight to cudaMemcpyAsync.
+  void h2d(void* dst, const void* src, size_t bytes);
+  void d2h(void* dst, const void* src, size_t bytes);
+
   // Per-kernel CUDA-event timing on this device's stream (off by default).
   bool profiling = false;
   cudaEvent_t prof_begin();
@@ -97,6 +107,9 @@ class Device {
   uint32_t* d_err_ = nullptr;
   void* d_scratch_ = nullptr;
   size_t scratch_cap_ = 0;
+  void* pin_[2] = {nullptr, nullptr};
+  cudaEvent_t pin_ev_[2] = {nullptr, nullptr};
+  void ensure_pinned();
   void* raw_alloc(size_t bytes);
   struct ProfRec { const char* name; cudaEvent_t a, b; };
   std::vector<ProfRec> prof_pending_;

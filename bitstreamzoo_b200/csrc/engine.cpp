@@ -6,12 +6,20 @@
 #include <functional>
 
 #include "fused.h"
+#include "vm.h"
 
 namespace bsz {
 namespace {
 
 constexpr int kMaxWhileIters = 10000;          // simulator/pythonsim/interpreter.py:20
 constexpr int64_t kSlotChunk = 1 << 16;
+// A straight-line run longer than this (unrolled loop nests reach tens of
+// millions of operations) is flushed at the next statement boundary, which
+// bounds host memory and lets the device work while the walk continues.
+constexpr size_t kAutoFlushNodes = size_t(1) << 20;
+// Segments with more operations than this never become one generated
+// kernel: NVRTC time and register pressure grow with the segment.
+constexpr size_t kMaxFusedOps = 3000;
 
 using Bits = std::vector<uint64_t>;
 inline bool bit(const Bits& b, int i) { return (b[i >> 6] >> (i & 63)) & 1u; }
@@ -43,10 +51,9 @@ Executor::Executor(Device& dev, const Program& prog, int64_t bitlength, ExecOpti
   all_ones_ = mk_raw(NOp::AllOnes, -1, -1, 0, 1);
   // Inputs that are not bound read as ZERO (interpreter.py:232-238).
   for (int id : prog.inputs) var_[id] = zero_;
-  if (opt_.mode == ExecMode::Fused) {
-    opt_.simplify = true;
+  if (opt_.mode != ExecMode::Plain) opt_.simplify = true;
+  if (opt_.mode == ExecMode::Fused || opt_.mode == ExecMode::Auto)
     fused_ = std::make_unique<FusedBackend>(dev_, opt_);
-  }
   BSZ_CUDA(cudaMalloc(&d_flag_, 256));
   ++dev_.n_mallocs;
   compute_liveness();
@@ -56,6 +63,7 @@ Executor::~Executor() {
   cudaStreamSynchronize(dev_.stream());
   if (d_flag_) cudaFree(d_flag_);
   if (d_slots_) cudaFree(d_slots_);
+  if (vm_buf_) cudaFree(vm_buf_);
 }
 
 void Executor::set_schedule(const Schedule& s) {
@@ -345,7 +353,10 @@ bool Executor::nonzero(int node, const Stmt* at) {
 }
 
 void Executor::exec_block(const std::vector<Stmt>& v) {
-  for (const auto& s : v) exec(s);
+  for (const auto& s : v) {
+    exec(s);
+    if (!tracing_ && nodes_.size() > nodes_after_flush_ + kAutoFlushNodes) flush(nullptr, nullptr);
+  }
 }
 
 void Executor::exec(const Stmt& s) {
@@ -471,7 +482,19 @@ void Executor::flush(const Bits* live, int* extra) {
   for (auto& p : pending_pops_) seg.pops.push_back({p.first, p.second - slot_base_});
   if (!seg.order.empty() || !seg.pops.empty()) {
     ++n_segments;
-    if (opt_.mode == ExecMode::Fused) {
+    bool fuse = false, vm = false;
+    switch (opt_.mode) {
+      case ExecMode::Plain: break;
+      case ExecMode::Vm: vm = true; break;
+      case ExecMode::Fused: fuse = seg.order.size() <= kMaxFusedOps; break;
+      case ExecMode::Auto:
+        if (nw_ <= kVmMaxWords) vm = true;
+        else fuse = seg.order.size() <= kMaxFusedOps && fused_pays(seg);
+        break;
+    }
+    if (vm) {
+      run_vm(seg);
+    } else if (fuse) {
       for (int i : seg.inputs) const_ptr(i);
       fused_->run(nodes_, seg, N_, nw_, d_slots_, &compile_ms);
     } else {
@@ -555,6 +578,132 @@ void Executor::run_plain(const Segment& seg) {
   max_live_buffers = std::max(max_live_buffers, live_buffer_count());
 }
 
+// Auto mode, long streams: a generated kernel pays when it is already
+// compiled (in this process or in the on-disk cache), or when the segment's
+// per-op form would take longer than compiling it.  Per-op time: launch
+// (~4 us) plus 24 bytes per word at HBM speed; compile time ~60 ms plus
+// ~0.4 ms per operation.
+bool Executor::fused_pays(const Segment& seg) {
+  const double ops = static_cast<double>(seg.order.size() + seg.pops.size());
+  const double per_op_ms = 0.004 + 24.0 * static_cast<double>(nw_) / 6.5e9;
+  const double compile_ms_est = 60.0 + 0.4 * static_cast<double>(seg.order.size());
+  if (ops * per_op_ms > compile_ms_est) return true;
+  return fused_->all_compiled(nodes_, seg, N_);
+}
+
+void Executor::run_vm(const Segment& seg) {
+  const int n_nodes = static_cast<int>(nodes_.size());
+  constexpr int32_t kNone = INT32_MIN;
+  std::vector<int32_t> loc(n_nodes, kNone);
+  std::vector<const uint64_t*> ext;
+  auto ext_of = [&](const uint64_t* p) {
+    ext.push_back(p);
+    return -static_cast<int32_t>(ext.size());
+  };
+  for (int i : seg.inputs) loc[i] = ext_of(nodes_[i].buf ? nodes_[i].buf->p : const_ptr(i));
+  std::vector<uint8_t> is_out(n_nodes, 0);
+  for (int o : seg.outputs) is_out[o] = 1;
+  std::vector<int64_t> last(n_nodes, -1);
+  for (size_t t = 0; t < seg.order.size(); ++t) {
+    const Node& x = nodes_[seg.order[t]];
+    if (x.a >= 0) last[x.a] = static_cast<int64_t>(t);
+    if (x.b >= 0) last[x.b] = static_cast<int64_t>(t);
+  }
+  // popcounts sorted by node (segment order is increasing node id)
+  std::vector<std::pair<int, int64_t>> pops(seg.pops.begin(), seg.pops.end());
+  std::stable_sort(pops.begin(), pops.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+  std::vector<VmOp> ops;
+  ops.reserve(seg.order.size() + pops.size());
+  auto emit_pops = [&](int node) {
+    auto it = std::lower_bound(pops.begin(), pops.end(), std::make_pair(node, int64_t(INT64_MIN)));
+    for (; it != pops.end() && it->first == node; ++it) {
+      VmOp op{};
+      op.code = kVmPop;
+      op.a = loc[node];
+      op.dst = static_cast<int32_t>(it->second);
+      ops.push_back(op);
+    }
+  };
+  for (int i : seg.inputs) emit_pops(i);
+  std::vector<int32_t> free_slots;
+  int32_t n_slots = 0;
+  const int64_t kmax = 64 * nw_;
+  for (size_t t = 0; t < seg.order.size(); ++t) {
+    const int id = seg.order[t];
+    Node& n = nodes_[id];
+    int32_t dst;
+    if (is_out[id]) {
+      n.buf = dev_.alloc_stream(nw_);
+      dst = ext_of(n.buf->p);
+    } else if (!free_slots.empty()) {
+      dst = free_slots.back();
+      free_slots.pop_back();
+    } else {
+      dst = n_slots++;
+    }
+    loc[id] = dst;
+    VmOp op{};
+    op.dst = dst;
+    op.a = loc[n.a];
+    switch (n.op) {
+      case NOp::Not: op.code = kVmNot; break;
+      case NOp::And: op.code = kVmAnd; op.b = loc[n.b]; break;
+      case NOp::Or: op.code = kVmOr; op.b = loc[n.b]; break;
+      case NOp::Xor: op.code = kVmXor; op.b = loc[n.b]; break;
+      case NOp::AndNot: op.code = kVmAndNot; op.b = loc[n.b]; break;
+      case NOp::Add: op.code = kVmAdd; op.b = loc[n.b]; break;
+      case NOp::Shl: op.code = kVmShl; op.b = static_cast<int32_t>(std::min<int64_t>(n.k, kmax)); break;
+      case NOp::Shr:
+        op.code = kVmShr;
+        op.b = static_cast<int32_t>(std::min<int64_t>(n.k, kmax));
+        op.fill = nodes_[n.a].tail ? 1 : 0;
+        break;
+      default: throw RuntimeError("internal: unexpected node in VM segment");
+    }
+    if (op.a == kNone || ((n.op == NOp::And || n.op == NOp::Or || n.op == NOp::Xor || n.op == NOp::AndNot ||
+                           n.op == NOp::Add) && op.b == kNone))
+      throw RuntimeError("internal: VM operand has no location");
+    ops.push_back(op);
+    emit_pops(id);
+    for (int operand : {n.a, n.b}) {
+      if (operand < 0 || loc[operand] < 0 || last[operand] != static_cast<int64_t>(t)) continue;
+      if (operand == n.b && n.a == n.b) continue;   // x op x: free once
+      free_slots.push_back(loc[operand]);
+    }
+    if (!is_out[id] && last[id] < 0) free_slots.push_back(dst);   // computed only for its popcounts
+  }
+  if (ops.empty()) return;
+  // device copies: instruction list | pointer table | slot file (if global)
+  auto align = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t ops_b = ops.size() * sizeof(VmOp);
+  const size_t ext_b = std::max<size_t>(1, ext.size()) * sizeof(uint64_t*);
+  const bool smem = vm_smem_bytes(n_slots, nw_) > 0;
+  const size_t file_b = smem ? 0 : static_cast<size_t>(n_slots) * static_cast<size_t>(nw_) * 8;
+  const size_t total = align(ops_b) + align(ext_b) + file_b;
+  if (total > vm_cap_) {
+    if (vm_buf_) {
+      BSZ_CUDA(cudaStreamSynchronize(dev_.stream()));
+      BSZ_CUDA(cudaFree(vm_buf_));
+      vm_buf_ = nullptr;
+    }
+    vm_cap_ = std::max<size_t>(total, size_t(1) << 20);
+    BSZ_CUDA(cudaMalloc(&vm_buf_, vm_cap_));
+    ++dev_.n_mallocs;
+  }
+  char* base = static_cast<char*>(vm_buf_);
+  VmOp* d_ops = reinterpret_cast<VmOp*>(base);
+  const uint64_t** d_ext = reinterpret_cast<const uint64_t**>(base + align(ops_b));
+  uint64_t* d_file = smem ? nullptr : reinterpret_cast<uint64_t*>(base + align(ops_b) + align(ext_b));
+  BSZ_CUDA(cudaMemcpyAsync(d_ops, ops.data(), ops_b, cudaMemcpyHostToDevice, dev_.stream()));
+  if (!ext.empty())
+    BSZ_CUDA(cudaMemcpyAsync(d_ext, ext.data(), ext.size() * sizeof(uint64_t*), cudaMemcpyHostToDevice,
+                             dev_.stream()));
+  VmLaunch L{d_ops, static_cast<int64_t>(ops.size()), d_ext, d_file, n_slots, nw_, last_mask_, d_slots_};
+  launch_vm(dev_, L);
+  ++vm_launches;
+  max_live_buffers = std::max(max_live_buffers, live_buffer_count() + n_slots);
+}
+
 void Executor::compact(int* extra) {
   std::vector<Node> old;
   old.swap(nodes_);
@@ -583,6 +732,7 @@ void Executor::compact(int* extra) {
   for (auto& a : arrs_)
     if (a) for (auto& kv : a->elems) kv.second = map(kv.second);
   if (extra) *extra = map(*extra);
+  nodes_after_flush_ = nodes_.size();
 }
 
 // ----------------------------------------------------------------- slots ---

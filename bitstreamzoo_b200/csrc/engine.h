@@ -46,7 +46,12 @@ struct Node {
   BufRef buf;             // Buf nodes, and computed nodes once materialized
 };
 
-enum class ExecMode : int { Plain = 0, Fused = 1 };
+// Plain: one kernel per operation.  Fused: generated segment kernels
+// (NVRTC).  Vm: each segment is one launch of the device interpreter
+// (vm.cu).  Auto: the VM for short streams; for long ones fused kernels when
+// they are cached or the segment's per-op time would exceed their compile
+// time, else per-op kernels.
+enum class ExecMode : int { Plain = 0, Fused = 1, Auto = 2, Vm = 3 };
 
 // Fused-kernel schedule: the knobs the autotuner and the cost model choose.
 struct Schedule {
@@ -104,6 +109,7 @@ class Executor {
   int64_t n_syncs = 0;
   int64_t max_live_buffers = 0;
   double compile_ms = 0.0;
+  int64_t vm_launches = 0;
   int64_t fused_launches() const;
   int64_t fused_fallbacks() const;
   void set_schedule(const Schedule& s);
@@ -167,6 +173,9 @@ class Executor {
 
   std::unique_ptr<FusedBackend> fused_;
   unsigned int* d_flag_ = nullptr;
+  void* vm_buf_ = nullptr;        // VM instruction list, pointer table and slot file
+  size_t vm_cap_ = 0;
+  size_t nodes_after_flush_ = 0;  // node count after the last compaction
   bool tracing_ = false;   // symbolic walk for batches: no device work, no length-dependent folds
 
   // walk
@@ -191,6 +200,8 @@ class Executor {
   void flush(const std::vector<uint64_t>* live, int* extra);
   void compact(int* extra);
   void run_plain(const Segment& seg);
+  void run_vm(const Segment& seg);
+  bool fused_pays(const Segment& seg);
   const uint64_t* const_ptr(int node);
   void ensure_slots(int64_t need);
   void resolve_slots();

@@ -166,6 +166,21 @@ struct Gen {
   std::set<int> in_part;           // computed in this part
   std::set<int> shl_src;           // temporaries shifted left (need previous-step value)
   std::map<int, int> shl_ws;       // max word shift per shl source temporary
+  // Shifted temporaries whose every left shift is by 1 or 2 bits: the bits
+  // shifted in come from the top bits of the word below, which one ballot
+  // per bit delivers to every lane; across steps only those 1-2 bits of the
+  // last lane are carried (a warp-uniform u32 instead of a 64-bit
+  // previous-step value per lane, and no shuffles).
+  std::map<int, int> small_shl;    // source -> max bit shift (1 or 2); absent: general
+  // Warp-uniform carried bits (add carries, small-shift edge bits) are packed
+  // into u32 words pk0, pk1, ...: bit position per add / small-shift source.
+  std::map<int, int> cbit, mbit;
+  int n_pack = 0;
+  // Emission order: depth-first from the part's roots, larger operand
+  // subtree first, which keeps fewer values live inside a step than node-id
+  // order (fewer registers, so more warps per SM).
+  std::vector<int> emit_order;
+  std::string pk(int bitpos) const { return "pk" + std::to_string(bitpos / 32); }
   std::vector<uint8_t> dyn;        // node dirt must be tracked during warm-up
   std::map<int, int64_t> sdh;      // static dirt (words) for nodes without add ancestors
   int64_t warm = 64;               // warm-up words
@@ -248,6 +263,13 @@ struct Gen {
       if (x.op == NOp::Add) dy = true;
       if (x.op == NOp::Shl && x.a >= 0 && in_part.count(x.a)) {
         int ws = static_cast<int>(x.k / 64);
+        const bool small = x.k >= 1 && x.k <= 2;
+        if (!shl_src.count(x.a)) {
+          if (small) small_shl[x.a] = static_cast<int>(x.k);
+        } else if (small_shl.count(x.a)) {
+          if (small) small_shl[x.a] = std::max(small_shl[x.a], static_cast<int>(x.k));
+          else small_shl.erase(x.a);
+        }
         shl_src.insert(x.a);
         shl_ws[x.a] = std::max(shl_ws[x.a], ws);
         s = d(x.a) + ws + ((x.k % 64) ? 1 : 0);
@@ -260,7 +282,65 @@ struct Gen {
     }
     warm = ((max_static + 64 + 31) / 32) * 32;
     if (warm > 8192) warm = 8192;
+    int nb = 0;
+    for (int n : part.order)
+      if (nodes[n].op == NOp::Add) cbit[n] = nb++;
+    for (auto& kv : small_shl) {
+      if (nb / 32 != (nb + kv.second - 1) / 32) nb = (nb / 32 + 1) * 32;   // keep a pair in one word
+      mbit[kv.first] = nb;
+      nb += kv.second;
+    }
+    n_pack = (nb + 31) / 32;
+    order_for_registers();
     make_slots();
+  }
+
+  void order_for_registers() {
+    std::map<int, int> users;
+    std::map<int, int64_t> size;
+    for (int n : part.order) {
+      const Node& x = nodes[n];
+      int64_t sz = 1;
+      for (int o : {x.a, x.b})
+        if (o >= 0 && in_part.count(o)) {
+          ++users[o];
+          sz += size[o];
+        }
+      size[n] = std::min<int64_t>(sz, int64_t(1) << 40);
+    }
+    std::set<int> seen;
+    emit_order.clear();
+    // iterative post-order DFS
+    auto visit = [&](int root) {
+      std::vector<std::pair<int, int>> st{{root, 0}};
+      while (!st.empty()) {
+        auto& [n, stage] = st.back();
+        if (stage == 0) {
+          if (seen.count(n)) { st.pop_back(); continue; }
+          seen.insert(n);
+          stage = 1;
+          const Node& x = nodes[n];
+          std::vector<int> kids;
+          for (int o : {x.a, x.b})
+            if (o >= 0 && in_part.count(o) && !seen.count(o)) kids.push_back(o);
+          if (kids.size() == 2 && size[kids[0]] < size[kids[1]]) std::swap(kids[0], kids[1]);
+          // push in reverse so the larger subtree is visited first
+          for (auto it = kids.rbegin(); it != kids.rend(); ++it) st.push_back({*it, 0});
+        } else {
+          emit_order.push_back(n);
+          st.pop_back();
+        }
+      }
+    };
+    std::vector<int> roots;
+    for (auto& o : outs) roots.push_back(o.first);
+    for (auto& p : part.pops) roots.push_back(p.first);
+    for (int n : part.order)
+      if (!users.count(n)) roots.push_back(n);
+    for (int r : roots)
+      if (in_part.count(r)) visit(r);
+    for (int n : part.order)
+      if (!seen.count(n)) visit(n);
   }
 
   // expression for an input node value at word index expression `idx`
@@ -289,7 +369,7 @@ struct Gen {
     if (!prefetched) emit_loads(s, "cur", true, "w", "base", "      ");
     for (auto& kv : in_idx) s << "      const u64 " << v(kv.first) << " = " << slot_cur(t_word(kv.first)) << ";\n";
     if (track) s << "      const int rel = (int)(base - p0);\n";
-    for (int n : part.order) {
+    for (int n : emit_order) {
       const Node& x = nodes[n];
       const std::string a = x.a >= 0 ? opnd(x.a) : "", b = x.b >= 0 ? opnd(x.b) : "";
       switch (x.op) {
@@ -303,7 +383,6 @@ struct Gen {
           s << "      u64 " << v(n) << " = " << a << " & ~" << b << ";\n";
           break;
         case NOp::Add: {
-          std::string c = "c" + std::to_string(n);
           s << "      u64 " << v(n) << ";\n      {\n"
             << "        const u64 sa = " << a << " + " << b << ";\n"
             << "        const u32 G = __ballot_sync(~0u, sa < " << a << ");\n"
@@ -317,9 +396,12 @@ struct Gen {
               << "          }\n"
               << "        }\n";
           }
-          s << "        const unsigned long long z = (unsigned long long)(G | P) + G + " << c << ";\n"
+          const int cb = cbit.at(n);
+          const std::string w = pk(cb), sh = std::to_string(cb % 32);
+          s << "        const unsigned long long z = (unsigned long long)(G | P) + G + ((" << w << " >> " << sh
+            << ") & 1u);\n"
             << "        const u32 cv = (u32)z ^ P;\n"
-            << "        " << c << " = (u32)(z >> 32);\n"
+            << "        " << w << " = (" << w << " & ~(1u << " << sh << ")) | ((u32)(z >> 32) << " << sh << ");\n"
             << "        " << v(n) << " = sa + ((cv >> lane) & 1u)" << (masked ? " & lm" : "") << ";\n"
             << "      }\n";
           break;
@@ -336,6 +418,20 @@ struct Gen {
                 << "        " << v(n) << " = (lo << " << bs << ") | (hi >> " << (64 - bs) << ");\n";
             } else {
               s << "        " << v(n) << " = lo;\n";
+            }
+            s << "      }\n";
+          } else if (small_shl.count(x.a)) {
+            const std::string cur = opnd(x.a), q = "q" + std::to_string(x.a);
+            const int mb = mbit.at(x.a);
+            const std::string w = pk(mb), sh = std::to_string(mb % 32), sh1 = std::to_string(mb % 32 + 1);
+            s << "      u64 " << v(n) << ";\n      {\n"
+              << "        const u32 m63 = (" << q << "_63 << 1) | ((" << w << " >> " << sh << ") & 1u);\n";
+            if (bs == 1) {
+              s << "        " << v(n) << " = (" << cur << " << 1) | (u64)((m63 >> lane) & 1u);\n";
+            } else {
+              s << "        const u32 m62 = (" << q << "_62 << 1) | ((" << w << " >> " << sh1 << ") & 1u);\n"
+                << "        " << v(n) << " = (" << cur << " << 2) | (u64)(((m63 >> lane) & 1u) << 1) | "
+                << "(u64)((m62 >> lane) & 1u);\n";
             }
             s << "      }\n";
           } else {
@@ -393,9 +489,29 @@ struct Gen {
           s << "      dh" << n << " = max(" << dh(x.a) << ", " << dh(x.b) << ");\n";
         }
       }
+      auto sm = small_shl.find(n);
+      if (sm != small_shl.end()) {
+        s << "      const u32 q" << n << "_63 = __ballot_sync(~0u, (" << v(n) << " >> 63) != 0ull);\n";
+        if (sm->second == 2)
+          s << "      const u32 q" << n << "_62 = __ballot_sync(~0u, ((" << v(n) << " >> 62) & 1ull) != 0ull);\n";
+      }
     }
-    // carry previous-step values of left-shifted temporaries
-    for (int n : shl_src) s << "      pv" << n << " = " << v(n) << ";\n";
+    // carry previous-step values of left-shifted temporaries (for 1-2 bit
+    // shifts only the last lane's top bits)
+    for (int n : shl_src) {
+      auto sm = small_shl.find(n);
+      if (sm == small_shl.end()) {
+        s << "      pv" << n << " = " << v(n) << ";\n";
+      } else {
+        const int mb = mbit.at(n);
+        const std::string w = pk(mb), sh = std::to_string(mb % 32);
+        const unsigned mask = sm->second == 2 ? 3u : 1u;
+        s << "      " << w << " = (" << w << " & ~(" << mask << "u << " << sh << ")) | ((q" << n << "_63 >> 31) << "
+          << sh << ")";
+        if (sm->second == 2) s << " | ((q" << n << "_62 >> 31) << " << (mb % 32 + 1) << ")";
+        s << ";\n";
+      }
+    }
     if (!track) {
       s << "      if (w < e) {\n";
       for (auto& kv : outs)
@@ -459,8 +575,9 @@ struct Gen {
     std::vector<int> adds;
     for (int n : part.order)
       if (nodes[n].op == NOp::Add) adds.push_back(n);
-    for (int n : adds) s << "  u32 c" << n << " = 0;\n";
-    for (int n : shl_src) s << "  u64 pv" << n << " = 0;\n";
+    for (int i = 0; i < n_pack; ++i) s << "  u32 pk" << i << " = 0;\n";
+    for (int n : shl_src)
+      if (!small_shl.count(n)) s << "  u64 pv" << n << " = 0;\n";
     for (size_t j = 0; j < part.pops.size(); ++j) s << "  u32 pc" << j << " = 0;\n";
     // ---- warm-up (speculative, exactness-checked)
     const bool need_warm = !adds.empty() || !shl_src.empty();
@@ -468,8 +585,9 @@ struct Gen {
       s << "  const long long H = " << warm << ";\n"
         << "  long long p0 = s - H;\n  if (p0 < 0) p0 = 0;\n"
         << "  for (int attempt = 0; p0 < s; ++attempt) {\n";
-      for (int n : adds) s << "    c" << n << " = 0;\n";
-      for (int n : shl_src) s << "    pv" << n << " = 0;\n";
+      for (int i = 0; i < n_pack; ++i) s << "    pk" << i << " = 0;\n";
+      for (int n : shl_src)
+        if (!small_shl.count(n)) s << "    pv" << n << " = 0;\n";
       for (int n : adds)
         if (dyn[n]) s << "    int res" << n << " = (p0 == 0);\n    int dh" << n << " = (p0 == 0) ? 0 : (1 << 30);\n";
       for (int n : part.order)
@@ -582,6 +700,21 @@ void disk_cache_store(const std::string& src, const std::string& cubin) {
       std::rename(tmp.c_str(), (base + ext).c_str());
     }
   }
+}
+
+// True when `src` is compiled in this process or present in the disk cache.
+bool is_compiled(const std::string& src) {
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    if (cache().count(src)) return true;
+  }
+  const std::string dir = cache_dir();
+  if (dir.empty()) return false;
+  const std::string base = dir + "/" + cache_key(src);
+  FILE* f = std::fopen((base + ".cubin").c_str(), "rb");
+  if (!f) return false;
+  std::fclose(f);
+  return read_file(base + ".cu") == src;
 }
 
 Compiled compile_source(const std::string& src, int block_threads, double* compile_ms,
@@ -699,6 +832,18 @@ std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg, bool
 }
 
 }  // namespace
+
+bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& seg, int64_t N) {
+  const Schedule& sc = impl_->opt.sched;
+  std::vector<Part> parts = split(nodes, seg, sc.cut_adds != 0);
+  for (Part& p : parts) {
+    if (p.order.empty() && p.pops.empty()) continue;
+    if (p.inputs.size() > kMaxInputs) return false;
+    Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
+    if (!is_compiled(g.source())) return false;
+  }
+  return true;
+}
 
 void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, int64_t nw,
                        unsigned long long* d_slots, double* compile_ms) {

@@ -23,6 +23,9 @@ class FusedBackend {
            unsigned long long* d_slots, double* compile_ms);
 
   void set_schedule(const Schedule& s);
+  // True when every kernel `run` would launch for this segment is already
+  // compiled (in this process or in the on-disk kernel cache).
+  bool all_compiled(const std::vector<Node>& nodes, const Segment& seg, int64_t N);
 
   int64_t fallbacks = 0;   // parts re-run with the plain kernels (speculation unproven)
   int64_t launches = 0;    // fused kernels launched

@@ -1,7 +1,13 @@
 // Host I/O implementation (see io.h).
 #include "io.h"
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <array>
 #include <cerrno>
 #include <chrono>
 #include <unordered_map>
@@ -9,6 +15,7 @@
 #include <cstring>
 #include <fstream>
 #include <stdexcept>
+#include <thread>
 
 #include "device.h"
 #include "engine.h"
@@ -198,6 +205,23 @@ void hex_to_words(const std::string& hex, std::vector<uint64_t>& w, uint8_t& tai
   }
 }
 
+uint64_t StreamVal::word(size_t i) const {
+  if (!view) return i < words.size() ? words[i] : 0;
+  if (i * 8 >= view_bytes) return 0;
+  uint64_t x = 0;
+  std::memcpy(&x, view + i * 8, std::min<size_t>(8, view_bytes - i * 8));
+  return x;
+}
+
+void StreamVal::materialize() {
+  if (!view) return;
+  words.assign(view_words, 0);
+  std::memcpy(words.data(), view, view_bytes);
+  view = nullptr;
+  view_bytes = view_words = 0;
+  hold.reset();
+}
+
 void words_to_hex(const uint64_t* w, size_t n, std::string& out) {
   static const char* digits = "0123456789abcdef";
   size_t top = n;
@@ -211,10 +235,37 @@ void words_to_hex(const uint64_t* w, size_t n, std::string& out) {
   out.resize(start + nd + 16 * (top - 1));
   char* o = &out[start];
   for (int k = nd - 1; k >= 0; --k) *o++ = digits[(t >> (4 * k)) & 15];
-  for (size_t i = top - 1; i > 0; --i) {
-    uint64_t x = w[i - 1];
-    for (int k = 15; k >= 0; --k) *o++ = digits[(x >> (4 * k)) & 15];
+  // full words: 16 digits each, most significant word first, two digits per
+  // byte from a 256-entry table; long outputs are split across threads
+  static const std::array<uint16_t, 256> pairs = [] {
+    std::array<uint16_t, 256> p{};
+    for (int b = 0; b < 256; ++b)
+      p[b] = static_cast<uint16_t>(static_cast<uint8_t>(digits[b >> 4]) |
+                                   (static_cast<uint16_t>(static_cast<uint8_t>(digits[b & 15])) << 8));
+    return p;
+  }();
+  const size_t full = top - 1;
+  auto encode = [&](size_t lo, size_t hi) {   // output words [lo, hi) in print order
+    for (size_t j = lo; j < hi; ++j) {
+      const uint64_t x = w[full - 1 - j];
+      char* d = o + 16 * j;
+      for (int b = 7; b >= 0; --b) {
+        const uint16_t pr = pairs[(x >> (8 * b)) & 0xff];
+        std::memcpy(d + 2 * (7 - b), &pr, 2);
+      }
+    }
+  };
+  const size_t kPerThread = size_t(1) << 18;   // 2 MiB of words
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>({static_cast<size_t>(hw), size_t(16), full / kPerThread});
+  if (nt <= 1) {
+    encode(0, full);
+    return;
   }
+  std::vector<std::thread> th;
+  const size_t per = (full + nt - 1) / nt;
+  for (size_t t0 = 0; t0 < full; t0 += per) th.emplace_back(encode, t0, std::min(full, t0 + per));
+  for (auto& t2 : th) t2.join();
 }
 
 // ---------------------------------------------------------------- bsdata ---
@@ -224,12 +275,19 @@ size_t words_for(int64_t bitlength) {
   return bitlength > 0 ? static_cast<size_t>((bitlength + 63) / 64) : 1;
 }
 
+// The mapping every view of the file being decoded points into.
+thread_local std::shared_ptr<const void> t_hold;
+
 StreamVal from_bytes(const uint8_t* bin, size_t bin_len, size_t off, size_t nbytes, size_t nw) {
   StreamVal v;
-  v.words.assign(nw, 0);
-  if (off + nbytes > bin_len) return v;   // out-of-range reference: zero (bsdata_reader.h:87-89)
-  size_t take = std::min(nbytes, nw * 8);
-  std::memcpy(v.words.data(), bin + off, take);
+  if (off + nbytes > bin_len) {   // out-of-range reference: zero (bsdata_reader.h:87-89)
+    v.words.assign(nw, 0);
+    return v;
+  }
+  v.view = bin + off;
+  v.view_bytes = std::min(nbytes, nw * 8);
+  v.view_words = nw;
+  v.hold = t_hold;
   return v;
 }
 
@@ -325,30 +383,55 @@ CaseInput parse_case(const JVal& h, const uint8_t* bin, size_t bin_len) {
 
 }  // namespace
 
+namespace {
+
+// A read-only private mapping of a whole file (unmapped when the last view
+// into it goes away).
+struct Mapping {
+  void* p = MAP_FAILED;
+  size_t n = 0;
+  ~Mapping() {
+    if (p != MAP_FAILED && n) munmap(p, n);
+  }
+};
+
+}  // namespace
+
 std::vector<CaseInput> read_bsdata(const std::string& path) {
-  std::FILE* f = std::fopen(path.c_str(), "rb");
-  if (!f) throw std::runtime_error("Cannot open bsdata file: " + path);
-  std::fseek(f, 0, SEEK_END);
-  long size = std::ftell(f);
-  std::fseek(f, 0, SEEK_SET);
-  std::vector<uint8_t> raw(static_cast<size_t>(std::max(size, 0L)));
-  size_t got = raw.empty() ? 0 : std::fread(raw.data(), 1, raw.size(), f);
-  std::fclose(f);
-  if (got != raw.size()) throw std::runtime_error("short read: " + path);
-  auto sep = std::find(raw.begin(), raw.end(), 0);
-  if (sep == raw.end()) throw std::runtime_error("Invalid bsdata file (no NUL separator): " + path);
-  size_t hlen = static_cast<size_t>(sep - raw.begin());
-  JVal h = json_parse(reinterpret_cast<const char*>(raw.data()), hlen);
-  const uint8_t* bin = raw.data() + hlen + 1;
-  size_t bin_len = raw.size() - hlen - 1;
+  const int fd = open(path.c_str(), O_RDONLY);
+  if (fd < 0) throw std::runtime_error("Cannot open bsdata file: " + path);
+  struct stat st;
+  if (fstat(fd, &st) != 0) {
+    close(fd);
+    throw std::runtime_error("Cannot stat bsdata file: " + path);
+  }
+  auto map = std::make_shared<Mapping>();
+  map->n = static_cast<size_t>(st.st_size);
+  if (map->n) map->p = mmap(nullptr, map->n, PROT_READ, MAP_PRIVATE, fd, 0);
+  close(fd);
+  if (map->n && map->p == MAP_FAILED) throw std::runtime_error("Cannot map bsdata file: " + path);
+  const uint8_t* raw = map->n ? static_cast<const uint8_t*>(map->p) : nullptr;
+  const uint8_t* sep = raw ? static_cast<const uint8_t*>(std::memchr(raw, 0, map->n)) : nullptr;
+  if (!sep) throw std::runtime_error("Invalid bsdata file (no NUL separator): " + path);
+  size_t hlen = static_cast<size_t>(sep - raw);
+  JVal h = json_parse(reinterpret_cast<const char*>(raw), hlen);
+  const uint8_t* bin = raw + hlen + 1;
+  size_t bin_len = map->n - hlen - 1;
+  t_hold = map;
   std::vector<CaseInput> cases;
   const JVal* multi = h.get("cases");
   if (!multi) multi = h.get("layers");
-  if (multi) {
-    for (auto& e : multi->a) cases.push_back(parse_case(e, bin, bin_len));
-  } else {
-    cases.push_back(parse_case(h, bin, bin_len));
+  try {
+    if (multi) {
+      for (auto& e : multi->a) cases.push_back(parse_case(e, bin, bin_len));
+    } else {
+      cases.push_back(parse_case(h, bin, bin_len));
+    }
+  } catch (...) {
+    t_hold.reset();
+    throw;
   }
+  t_hold.reset();
   if (cases.size() == 1) {
     cases[0].name = path;
   } else {
@@ -368,8 +451,22 @@ namespace {
 
 BufRef upload(Device& dev, const StreamVal& v, int64_t nw) {
   BufRef b = dev.alloc_stream(nw);
-  size_t have = std::min<size_t>(v.words.size(), static_cast<size_t>(nw));
-  if (have) BSZ_CUDA(cudaMemcpyAsync(b->p, v.words.data(), have * 8, cudaMemcpyHostToDevice, dev.stream()));
+  size_t have = std::min<size_t>(v.n_words(), static_cast<size_t>(nw));
+  if (have && v.view) {
+    // whole words straight from the mapping; a partial last word and the
+    // zero words after the stored bytes are filled from a padded copy
+    const size_t bytes = std::min(v.view_bytes, have * 8);
+    const size_t whole = bytes / 8;
+    dev.h2d(b->p, v.view, whole * 8);
+    if (whole < have) {
+      std::vector<uint64_t> rest(have - whole, 0);
+      std::memcpy(rest.data(), v.view + whole * 8, bytes - whole * 8);
+      BSZ_CUDA(cudaMemcpyAsync(b->p + whole, rest.data(), rest.size() * 8, cudaMemcpyHostToDevice, dev.stream()));
+      BSZ_CUDA(cudaStreamSynchronize(dev.stream()));   // `rest` is a local
+    }
+  } else if (have) {
+    dev.h2d(b->p, v.words.data(), have * 8);
+  }
   if (static_cast<int64_t>(have) < nw) {
     uint64_t fill = v.tail ? ~uint64_t(0) : 0;
     launch_fill(dev, b->p + have, nw - static_cast<int64_t>(have), fill, fill);
@@ -381,21 +478,24 @@ bool is_clean(const StreamVal& v, int64_t N, int64_t nw) {
   if (v.tail) return false;
   int64_t lw = (N + 63) / 64;
   if (lw <= 0) return true;
-  if (static_cast<int64_t>(v.words.size()) >= lw) {
-    uint64_t hi = v.words[lw - 1] & ~mask_for_bits(N);
+  const size_t n = v.n_words();
+  if (static_cast<int64_t>(n) >= lw) {
+    uint64_t hi = v.word(static_cast<size_t>(lw - 1)) & ~mask_for_bits(N);
     if (hi) return false;
   }
-  for (size_t i = static_cast<size_t>(lw); i < v.words.size() && static_cast<int64_t>(i) < nw; ++i)
-    if (v.words[i]) return false;
+  for (size_t i = static_cast<size_t>(lw); i < n && static_cast<int64_t>(i) < nw; ++i)
+    if (v.word(i)) return false;
   return true;
 }
 
 void download(Device& dev, const BufRef& b, int64_t nw, std::vector<uint64_t>& out) {
   out.resize(nw);
-  BSZ_CUDA(cudaMemcpyAsync(out.data(), b->p, nw * 8, cudaMemcpyDeviceToHost, dev.stream()));
+  dev.d2h(out.data(), b->p, static_cast<size_t>(nw) * 8);
 }
 
 }  // namespace
+
+static const char* const kModeNames[4] = {"b200-plain", "b200-fused", "b200-auto", "b200-vm"};
 
 std::string run_case_json(Device& dev, const Program& prog, CaseInput& c, const DriverOptions& o,
                           double parse_ms) {
@@ -404,11 +504,11 @@ std::string run_case_json(Device& dev, const Program& prog, CaseInput& c, const 
   int64_t static_ops = count_static_ops(prog, pmap);
   int64_t nw = c.bitlength > 0 ? (c.bitlength + 63) / 64 : 1;
   if (c.bitlength <= 0)
-    for (auto& kv : c.inputs) nw = std::max<int64_t>(nw, static_cast<int64_t>(kv.second.words.size()));
+    for (auto& kv : c.inputs) nw = std::max<int64_t>(nw, static_cast<int64_t>(kv.second.n_words()));
   const int64_t N = c.bitlength > 0 ? c.bitlength : 64 * nw;
 
   ExecOptions eo;
-  eo.mode = o.mode == 1 ? ExecMode::Fused : ExecMode::Plain;
+  eo.mode = static_cast<ExecMode>(o.mode & 3);
 
   struct OutRec {
     std::map<std::string, std::pair<std::vector<uint64_t>, uint8_t>> streams;
@@ -567,7 +667,7 @@ std::string run_case_json(Device& dev, const Program& prog, CaseInput& c, const 
                 static_cast<long long>(launches), static_cast<long long>(dev.n_mallocs),
                 static_cast<long long>(dev.bytes_peak),
                 static_cast<long long>(max_live * nw * 8), gops,
-                o.mode == 1 ? "b200-fused" : "b200-plain", parse_ms, compile_ms, exec_ms, kernel_ms,
+                kModeNames[o.mode & 3], parse_ms, compile_ms, exec_ms, kernel_ms,
                 warm_ms);
   js += buf;
   return js;

@@ -44,9 +44,20 @@ std::string json_quote(const std::string& s);
 void hex_to_words(const std::string& hex, std::vector<uint64_t>& words, uint8_t& tail);
 void words_to_hex(const uint64_t* w, size_t n, std::string& out);   // appends "0x..."
 
+// A stream input: owned words (JSON inputs, fed-back outputs), or a view of
+// packed bytes inside a memory-mapped .bsdata file (no host copy; `hold`
+// keeps the mapping alive).  Either way the value has n_words() words,
+// zero past the stored bytes, and bits beyond them equal to `tail`.
 struct StreamVal {
   std::vector<uint64_t> words;
+  const uint8_t* view = nullptr;
+  size_t view_bytes = 0;
+  size_t view_words = 0;
+  std::shared_ptr<const void> hold;
   uint8_t tail = 0;
+  size_t n_words() const { return view ? view_words : words.size(); }
+  uint64_t word(size_t i) const;
+  void materialize();   // view -> words
 };
 
 struct CaseInput {
@@ -70,7 +81,7 @@ struct Program;
 
 struct DriverOptions {
   bool warmup = false;
-  int mode = 0;   // 0 plain, 1 fused
+  int mode = 2;   // 0 plain, 1 fused, 2 auto, 3 vm (ExecMode)
 };
 
 // Runs one case end to end (H2D, execute, D2H) and returns the JSON object

@@ -125,7 +125,7 @@ __global__ void k_colsum(const float* __restrict__ d, float* __restrict__ g, int
 
 __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
                        float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps,
-                       float c1, float c2) {
+                       float c1, float c2, float wd) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float gi = g[i];
@@ -133,7 +133,8 @@ __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float
   float vi = b2 * v[i] + (1.f - b2) * gi * gi;
   m[i] = mi;
   v[i] = vi;
-  w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  // decoupled weight decay (AdamW): w <- w - lr * (mhat / (sqrt(vhat) + eps) + wd * w)
+  w[i] -= lr * ((mi / c1) / (sqrtf(vi / c2) + eps) + wd * w[i]);
 }
 
 void check(cudaError_t e, const char* what) {
@@ -259,7 +260,8 @@ float Mlp::train_step(const float* x, const float* y, int n, float lr) {
   const float c1 = 1.f - std::pow(b1, static_cast<float>(step_));
   const float c2 = 1.f - std::pow(b2, static_cast<float>(step_));
   k_adam<<<static_cast<unsigned>((n_params_ + 255) / 256), 256, 0, stream_>>>(w_, g_, m_, v_, n_params_, lr,
-                                                                                b1, b2, 1e-8f, c1, c2);
+                                                                                b1, b2, 1e-8f, c1, c2,
+                                                                                weight_decay_);
   check(cudaGetLastError(), "mlp adam");
   ++launches;
   return loss;

@@ -23,6 +23,7 @@ class Mlp {
   // Loss and gradient of the loss w.r.t. the flat parameters (no update).
   float gradients(const float* x, const float* y, int n, float* grad);
   void get_params(float* out) const;
+  void set_weight_decay(float wd) { weight_decay_ = wd; }
   void set_params(const float* in);
   int64_t launches = 0;
 
@@ -40,6 +41,7 @@ class Mlp {
   std::vector<float*> act_, delta_;
   int cap_ = 0;
   int64_t step_ = 0;
+  float weight_decay_ = 0.f;
   cudaStream_t stream_;
   void ensure(int n);
   void upload(const float* x, const float* y, int n);

@@ -9,12 +9,18 @@
 #define __forceinline__ inline
 #endif
 
+#ifdef __CUDA_ARCH__
+#define BSZ_UNROLL _Pragma("unroll")
+#else
+#define BSZ_UNROLL
+#endif
+
 namespace bsz {
 
 // Transposes the 64 bytes in x[0..7] (x[q] = bytes 8q..8q+7) into the eight
 // basis words: afterwards x[i] bit (8q + k) = bit i of byte (8q + k).
 __host__ __device__ __forceinline__ void s2p_transpose64(uint64_t x[8]) {
-#pragma unroll
+BSZ_UNROLL
   for (int q = 0; q < 8; ++q) {
     uint64_t v = x[q], t;
     // bit (8r + c) <-> bit (8c + r)
@@ -27,13 +33,13 @@ __host__ __device__ __forceinline__ void s2p_transpose64(uint64_t x[8]) {
     x[q] = v;
   }
   // byte matrix transpose: row q, column i -> row i, column q
-#pragma unroll
+BSZ_UNROLL
   for (int q = 0; q < 4; ++q) {
     const uint64_t a = x[q], b = x[q + 4];
     x[q] = (a & 0x00000000FFFFFFFFull) | (b << 32);
     x[q + 4] = (a >> 32) | (b & 0xFFFFFFFF00000000ull);
   }
-#pragma unroll
+BSZ_UNROLL
   for (int h = 0; h < 4; ++h) {
     const int q = (h & 1) | ((h & 2) << 1);   // 0, 1, 4, 5
     const uint64_t a = x[q], b = x[q + 2];
@@ -41,7 +47,7 @@ __host__ __device__ __forceinline__ void s2p_transpose64(uint64_t x[8]) {
     x[q] = (a & m) | ((b & m) << 16);
     x[q + 2] = ((a >> 16) & m) | (b & ~m);
   }
-#pragma unroll
+BSZ_UNROLL
   for (int h = 0; h < 4; ++h) {
     const int q = 2 * h;
     const uint64_t a = x[q], b = x[q + 1];

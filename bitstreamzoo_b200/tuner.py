@@ -44,7 +44,7 @@ from . import DEFAULT_SCHEDULE, MODE_FUSED, BszError
 
 # Knobs that change the generated code (one NVRTC compile each) and knobs
 # that only change the launch.
-CODEGEN_AXES = {"warps": (4, 8), "min_blocks": (2, 4), "prefetch": (0, 1), "cut_adds": (0, 1)}
+CODEGEN_AXES = {"warps": (4, 8), "min_blocks": (2, 4, 8), "prefetch": (0, 1), "cut_adds": (0, 1)}
 LAUNCH_AXES = {"ctas_per_sm": (0, 2)}
 
 
@@ -176,13 +176,15 @@ class CostModel:
     CUDA kernels.  Inputs are standardised with the training set's mean and
     standard deviation; the target is standardised log(ms)."""
 
-    def __init__(self, ctx, in_dim: int, hidden: int = 256, layers: int = 3, seed: int = 1):
+    def __init__(self, ctx, in_dim: int, hidden: int = 256, layers: int = 3, seed: int = 1,
+                 weight_decay: float = 0.0):
         self.ctx = ctx
         self.lib = ctx.lib
         self.in_dim = in_dim
         self.h = self.lib.bsz_mlp_create(ctx.h, in_dim, hidden, layers, seed)
         if not self.h:
             raise BszError(_lib.last_error())
+        self.set_weight_decay(weight_decay)
         self.mu = np.zeros(in_dim, np.float32)
         self.sd = np.ones(in_dim, np.float32)
         self.y_mu = 0.0
@@ -195,6 +197,9 @@ class CostModel:
                 self.h = None
         except Exception:
             pass
+
+    def set_weight_decay(self, wd: float):
+        _lib.check(self.lib.bsz_mlp_set_weight_decay(self.h, ctypes.c_float(wd)))
 
     # raw access (standardised units), used by the gradient checks
     @property
@@ -235,10 +240,20 @@ class CostModel:
         return float(loss.value)
 
     # standardised training and prediction
-    def fit(self, X, ms, steps: int = 1500, batch: int = 256, lr: float = 1e-3, seed: int = 0) -> list:
-        """Fits log(ms); returns the loss of every step."""
+    def fit(self, X, ms, steps: int = 1500, batch: int = 256, lr: float = 1e-3, seed: int = 0,
+            groups=None) -> list:
+        """Fits log(ms); returns the loss of every step.  With ``groups`` (one
+        label per row, e.g. the (program, length) case), the target is log(ms)
+        minus its group's mean: the model then learns how schedules rank
+        within a case, which is all a pick needs, instead of spending its
+        capacity on the cases' absolute times."""
         X = np.asarray(X, np.float32)
         y = np.log(np.asarray(ms, np.float64))
+        if groups is not None:
+            groups = np.asarray(groups)
+            for g in np.unique(groups):
+                sel = groups == g
+                y[sel] -= y[sel].mean()
         self.mu = X.mean(0)
         self.sd = np.maximum(X.std(0), 1e-3).astype(np.float32)
         self.y_mu = float(y.mean())
@@ -330,12 +345,22 @@ def _device_inputs(nbits: int, n_inputs: int, seed: int):
     return bufs, {f"b{i}": (b.data_ptr(), nw) for i, b in enumerate(bufs)}
 
 
+def codegen_key(s: dict) -> tuple:
+    return tuple(int(s[k]) for k in CODEGEN_AXES)
+
+
 def study(ctx, train_srcs, test_srcs, sizes=(1 << 23, 1 << 25, 1 << 27), candidates=None,
-          sample_frac: float = 0.25, reps: int = 3, steps: int = 1500, seed: int = 0, log=None) -> dict:
-    """Collects timings (a ``sample_frac`` sample of the candidates for each
-    training (program, length); every candidate for held-out ones), fits a
-    :class:`CostModel` and reports pick regret on the held-out programs for
-    the model's top-1 and top-4 picks and for the default schedule."""
+          sample_frac: float = 0.25, reps: int = 3, steps: int = 3000, seed: int = 0, log=None,
+          weight_decay: float = 1e-4) -> dict:
+    """Collects timings, fits a :class:`CostModel` and reports pick regret on
+    the held-out programs for the model's top-1 and top-4 picks and for the
+    default schedule.
+
+    Sampling budget: compiling a generated kernel costs far more than timing
+    it, so each training program draws a ``sample_frac`` share of the
+    code-generation variants (warps, register cap, prefetch, add cuts) and
+    times every launch variant of those at every length.  Held-out programs
+    are timed exhaustively (that is the regret's reference)."""
     import time as _time
 
     candidates = candidates or CANDIDATES
@@ -352,21 +377,27 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 23, 1 << 25, 1 << 27), candida
             progs[src] = (progs[src][0], program_features(progs[src][0]))
         return progs[src]
 
+    groups = []
+    variants = sorted({codegen_key(s) for s in candidates})
     for i, src in enumerate(train_srcs):
         prog, pf = prog_of(src)
+        k = max(1, int(round(sample_frac * len(variants))))
+        chosen = {variants[j] for j in rng.choice(len(variants), size=k, replace=False)}
         for n in sizes:
-            k = max(1, int(round(sample_frac * len(candidates))))
-            for j in rng.choice(len(candidates), size=k, replace=False):
-                ms = measure(ctx, prog, n, bufs_by_size[n][1], candidates[j], reps=reps)
-                X.append(feature_row(pf, n, candidates[j]))
+            for s in candidates:
+                if codegen_key(s) not in chosen:
+                    continue
+                ms = measure(ctx, prog, n, bufs_by_size[n][1], s, reps=reps)
+                X.append(feature_row(pf, n, s))
                 y.append(ms)
+                groups.append(i * 1000 + sizes.index(n))
                 n_timed += 1
         if log:
             log(f"train {i + 1}/{len(train_srcs)} timed={n_timed} t={_time.time() - t0:.0f}s")
     t_collect = _time.time() - t0
-    model = CostModel(ctx, len(X[0]), seed=seed + 1)
+    model = CostModel(ctx, len(X[0]), seed=seed + 1, weight_decay=weight_decay)
     t1 = _time.time()
-    losses = model.fit(X, y, steps=steps, seed=seed)
+    losses = model.fit(X, y, steps=steps, seed=seed, groups=groups)
     t_fit = _time.time() - t1
 
     default_key = schedule_key(DEFAULT_SCHEDULE)

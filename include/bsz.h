@@ -40,6 +40,10 @@ typedef struct bsz_run bsz_run;
 /* Execution forms. */
 #define BSZ_MODE_PLAIN 0   /* one kernel per DSL operation */
 #define BSZ_MODE_FUSED 1   /* whole straight-line segments as one generated kernel */
+#define BSZ_MODE_AUTO 2    /* device interpreter (one launch per segment) for streams of at
+                              most 8192 words; generated kernels for longer ones when cached
+                              or worth compiling; else one kernel per operation */
+#define BSZ_MODE_VM 3      /* every segment on the device interpreter */
 
 typedef struct bsz_stats {
   int64_t op_count;          /* dynamic DSL op count (same counting as the reference) */
@@ -53,6 +57,7 @@ typedef struct bsz_stats {
   double compile_ms;         /* time spent generating/compiling fused kernels */
   int64_t n_fused_launches;  /* generated segment kernels launched */
   int64_t n_fused_fallbacks; /* segment parts re-run per-op because speculation was unproven */
+  int64_t n_vm_launches;     /* segments run by the device interpreter */
 } bsz_stats;
 
 /* Schedule of the generated segment kernels (fused form).  The autotuner and
@@ -174,13 +179,15 @@ int bsz_mlp_gradients(bsz_mlp* mlp, const float* x, const float* y, int n, float
 /* Flat parameters W1 b1 W2 b2 ... Wout bout (each W row-major [fan_in, fan_out]);
  * get != 0 copies them out, get == 0 loads them (and resets Adam state). */
 int bsz_mlp_params(bsz_mlp* mlp, float* params, int get);
+/* Decoupled (AdamW) weight decay applied by bsz_mlp_train_step (default 0). */
+int bsz_mlp_set_weight_decay(bsz_mlp* mlp, float weight_decay);
 void bsz_mlp_free(bsz_mlp* mlp);
 
 /* ---- whole-case driver (replaces run_case<64>, main.cu:23-207) ----------
  * Runs `source` on every case of a .bsdata file (or, if bsdata_path is NULL,
  * on the JSON input document `json_input`, the stdin form of main.cu) and
  * returns the bsim_cuda JSON text (one object, or an array for multi-case
- * files).  flags: bit 0 = --warmup, bit 1 = fused mode.  The returned string
+ * files).  flags: bit 0 = --warmup, bits 1-2 = execution mode (BSZ_MODE_*).  The returned string
  * is owned by the library and valid until the next call on this thread. */
 const char* bsz_run_case_json(bsz_ctx* ctx, const char* source, const char* bsdata_path,
                               const char* json_input, int flags);

@@ -50,9 +50,9 @@ def loss_and_grad(params, dims, x, y):
     return loss, flat
 
 
-def adam_step(params, grad, m, v, step, lr, b1=0.9, b2=0.999, eps=1e-8):
+def adam_step(params, grad, m, v, step, lr, b1=0.9, b2=0.999, eps=1e-8, wd=0.0):
     m = b1 * m + (1 - b1) * grad
     v = b2 * v + (1 - b2) * grad * grad
     c1 = 1 - b1 ** step
     c2 = 1 - b2 ** step
-    return params - lr * (m / c1) / (np.sqrt(v / c2) + eps), m, v
+    return params - lr * ((m / c1) / (np.sqrt(v / c2) + eps) + wd * params), m, v

@@ -14,7 +14,7 @@ from conftest import expected_masked, load_golden, run_golden_case
 import bitstreamzoo_b200 as bz
 
 GROUPS = ["random_programs", "kat_ops", "tail_corners"]
-MODES = [bz.MODE_PLAIN, bz.MODE_FUSED]
+MODES = [bz.MODE_PLAIN, bz.MODE_FUSED, bz.MODE_VM, bz.MODE_AUTO]
 
 
 @pytest.mark.gpu

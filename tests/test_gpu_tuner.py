@@ -53,8 +53,10 @@ def test_mlp_gradients_match_numpy(ctx, n):
     assert err < 1e-4, err
 
 
-def test_mlp_adam_steps_match_numpy(ctx):
+@pytest.mark.parametrize("wd", [0.0, 0.05])
+def test_mlp_adam_steps_match_numpy(ctx, wd):
     m, dims = _model(ctx, in_dim=6, hidden=32, layers=2)
+    m.set_weight_decay(wd)
     rng = np.random.default_rng(3)
     p = m.params().astype(np.float64)
     mom = np.zeros_like(p)
@@ -63,7 +65,7 @@ def test_mlp_adam_steps_match_numpy(ctx):
         x = rng.normal(0, 1, (64, 6)).astype(np.float32)
         y = rng.normal(0, 1, 64).astype(np.float32)
         _, g = mlp_ref.loss_and_grad(p, dims, x.astype(np.float64), y.astype(np.float64))
-        p, mom, vel = mlp_ref.adam_step(p, g, mom, vel, step, 1e-3)
+        p, mom, vel = mlp_ref.adam_step(p, g, mom, vel, step, 1e-3, wd=wd)
         m.raw_train_step(x, y, 1e-3)
         np.testing.assert_allclose(m.params(), p, atol=2e-6, rtol=0)
 

@@ -4,6 +4,7 @@ the bsim_cuda driver reads .bsdata files (no GPU needed for any of this)."""
 
 import ctypes
 import json
+import random
 import os
 import re
 import subprocess
@@ -110,3 +111,24 @@ def test_cli_parse_error_exit_code(tmp_path):
                          capture_output=True, text=True, timeout=60)
     assert out.returncode == 1
     assert "Parse error" in out.stderr
+
+
+def test_cli_dump_input_large_stream_hex(tmp_path):
+    """A 5 MiB stream through the memory-mapped reader and the table-driven,
+    multi-threaded hex encoder (long outputs are split across threads), plus
+    a stream whose bytes end mid-word."""
+    exe = bz.bsim_cuda_path()
+    prog = tmp_path / "p.bs"
+    prog.write_text("input stream a\ninput stream b\noutput stream r\nr = a\n")
+    nbits = 5 * 8 * (1 << 20) + 21
+    rng = random.Random(5)
+    a = rng.getrandbits(nbits) | (1 << (nbits - 1))
+    b = rng.getrandbits(13 * 8 + 5)
+    path = tmp_path / "big.bsdata"
+    write_bsdata(str(path), nbits, inputs={"a": a, "b": b})
+    out = subprocess.run([exe, str(prog), "--input", str(path), "--dump-input"],
+                         capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr[-2000:]
+    d = json.loads(out.stdout)
+    assert d["inputs"]["a"] == hex(a)
+    assert int(d["inputs"]["b"], 16) == b
