@@ -56,6 +56,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-op comparison form")
+    ap.add_argument("--schedule", default="model", choices=["model", "default"],
+                    help="fused-kernel schedule: picked by the shipped cost model (no timing), or the default")
     return ap.parse_args()
 
 
@@ -313,8 +315,17 @@ def run_ours(args, rank, world, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    sched, sched_src = dict(bz.DEFAULT_SCHEDULE), "default"
+    if args.schedule == "model":
+        from bitstreamzoo_b200 import tuner
+        model = tuner.CostModel.load_default(ctx)
+        if model is not None:
+            sched, sched_src = model.choose(prog, nbits), "cost model (top-1, no timing)"
+
     def step(mode):
         r = prog.run(nbits, mode)
+        if mode == bz.MODE_FUSED:
+            r.set_schedule(sched)
         for k, t in dev_in.items():
             r.bind(k, ("borrow", t.data_ptr(), nw))
         st = r.execute()
@@ -443,6 +454,7 @@ def run_ours(args, rank, world, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": W.data,
             "config": {"workload": W.desc + " (per GPU)", "form": args.mode, "bits_per_stream": nbits,
+                       "schedule": sched, "schedule_source": sched_src,
                        "l2": ("inputs larger than L2; no flush needed" if W.in_bytes > (126 << 20)
                               else "inputs fit in L2 (reported, not roofline-judged)"),
                        "parallelism": f"replicas x{world} (independent stream sets)"},

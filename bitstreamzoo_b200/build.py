@@ -33,7 +33,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-Wall,-Wno-unus
           "-I", CSRC, "-I", os.path.join(ROOT, "include")]
 
 LIB_SOURCES = ["frontend.cpp", "device.cu", "kernels.cu", "engine.cpp", "fused.cpp", "io.cpp",
-               "capi.cpp", "noalloc.cu", "mlp.cu", "s2p.cu", "vm.cu"]
+               "capi.cpp", "noalloc.cu", "mlp.cu", "s2p.cu", "vm.cu", "vmprog.cpp"]
 MAIN_SOURCES = ["bsim_main.cpp"]
 HEADERS = ["frontend.h", "device.h", "engine.h", "fused.h", "io.h", "mlp.h", "s2p.h", "vm.h"]
 

@@ -94,6 +94,17 @@ int input_id(bsz_run* r, const char* name) {
   return -1;
 }
 
+// Page-locked (or managed) host memory copies at link speed directly;
+// pageable memory goes through the device's pinned staging buffers.
+bool is_pinned(const void* p) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost || at.type == cudaMemoryTypeManaged;
+}
+
 int name_id(bsz_run* r, const char* name) {
   int id = r->prog->prog->find(name ? name : "");
   if (id < 0) throw std::invalid_argument(std::string("unknown name: ") + (name ? name : "(null)"));
@@ -229,10 +240,14 @@ int bsz_bind_input(bsz_run* run, const char* name, int64_t index, const uint64_t
     }
     bsz::BufRef b = dev.alloc_stream(nw);
     const int64_t have = std::min<int64_t>(static_cast<int64_t>(n_words), nw);
-    if (have > 0)
-      BSZ_CUDA(cudaMemcpyAsync(b->p, words, have * 8,
-                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                               dev.stream()));
+    if (have > 0) {
+      if (on_device || is_pinned(words))
+        BSZ_CUDA(cudaMemcpyAsync(b->p, words, have * 8,
+                                 on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                 dev.stream()));
+      else
+        dev.h2d(b->p, words, static_cast<size_t>(have) * 8);   // pageable: staged
+    }
     if (have < nw) {
       uint64_t fill = tail ? ~uint64_t(0) : 0;
       bsz::launch_fill(dev, b->p + have, nw - have, fill, fill);
@@ -310,8 +325,12 @@ int bsz_get_stream(bsz_run* run, const char* name, int64_t index, uint64_t* host
     bsz::BufRef b = find_stream(run, name, index);
     const int64_t nw = words_of(run->bitlength);
     const int64_t n = std::min<int64_t>(nw, static_cast<int64_t>(n_words));
-    BSZ_CUDA(cudaMemcpyAsync(host, b->p, n * 8, cudaMemcpyDeviceToHost, dev.stream()));
-    dev.sync();
+    if (is_pinned(host)) {
+      BSZ_CUDA(cudaMemcpyAsync(host, b->p, n * 8, cudaMemcpyDeviceToHost, dev.stream()));
+      dev.sync();
+    } else {
+      dev.d2h(host, b->p, static_cast<size_t>(n) * 8);   // pageable: staged
+    }
     if (n == nw && run->bitlength > 0) host[nw - 1] &= bsz::mask_for_bits(run->bitlength);
   });
 }

@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <functional>
 
 #include "fused.h"
@@ -60,6 +62,13 @@ Executor::Executor(Device& dev, const Program& prog, int64_t bitlength, ExecOpti
 }
 
 Executor::~Executor() {
+  if (std::getenv("BSZ_HOST_TIMES"))
+    std::fprintf(stderr,
+                 "[bsz] segments=%lld vm=%lld fused=%lld ops=%lld host ms: segment %.2f policy %.2f run %.2f "
+                 "compact %.2f compile %.2f\n",
+                 static_cast<long long>(n_segments), static_cast<long long>(vm_launches),
+                 static_cast<long long>(fused_launches()), static_cast<long long>(op_count), t_segment_ms,
+                 t_policy_ms, t_run_ms, t_compact_ms, compile_ms);
   cudaStreamSynchronize(dev_.stream());
   if (d_flag_) cudaFree(d_flag_);
   if (d_slots_) cudaFree(d_slots_);
@@ -415,7 +424,26 @@ void Executor::exec(const Stmt& s) {
   }
 }
 
+namespace {
+bool has_control_flow(const std::vector<Stmt>& v) {
+  for (const auto& s : v) {
+    if (s.kind == Stmt::If || s.kind == Stmt::While) return true;
+    if (s.kind == Stmt::For && has_control_flow(s.body)) return true;
+  }
+  return false;
+}
+}  // namespace
+
 void Executor::run() {
+  // Programs with if/while on short streams: the whole program, branches
+  // included, runs as one launch of the device interpreter (no host round
+  // trip per condition) when it qualifies.
+  if (!tracing_ && has_control_flow(prog_.stmts) &&
+      (opt_.mode == ExecMode::Vm || (opt_.mode == ExecMode::Auto && nw_ <= kVmMaxWords)) &&
+      run_vm_program()) {
+    ran_as_vm_program = true;
+    return;
+  }
   exec_block(prog_.stmts);
   flush(&live_end_, nullptr);
   resolve_slots();
@@ -444,6 +472,9 @@ void Executor::flush(const Bits* live, int* extra) {
     throw RuntimeError("batch execution needs straight-line programs: this one needs the device "
                        "during the walk (a stream condition, or a popcount used as a loop bound, "
                        "index or shift amount)");
+  using clk = std::chrono::steady_clock;
+  auto ms_since = [](clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); };
+  auto t0 = clk::now();
   const int n_nodes = static_cast<int>(nodes_.size());
   std::vector<uint8_t> is_target(n_nodes, 0), need(n_nodes, 0);
   Segment seg;
@@ -480,8 +511,10 @@ void Executor::flush(const Bits* live, int* extra) {
     else seg.inputs.push_back(i);
   }
   for (auto& p : pending_pops_) seg.pops.push_back({p.first, p.second - slot_base_});
+  t_segment_ms += ms_since(t0);
   if (!seg.order.empty() || !seg.pops.empty()) {
     ++n_segments;
+    auto t1 = clk::now();
     bool fuse = false, vm = false;
     switch (opt_.mode) {
       case ExecMode::Plain: break;
@@ -492,6 +525,8 @@ void Executor::flush(const Bits* live, int* extra) {
         else fuse = seg.order.size() <= kMaxFusedOps && fused_pays(seg);
         break;
     }
+    t_policy_ms += ms_since(t1);
+    auto t2 = clk::now();
     if (vm) {
       run_vm(seg);
     } else if (fuse) {
@@ -500,10 +535,13 @@ void Executor::flush(const Bits* live, int* extra) {
     } else {
       run_plain(seg);
     }
+    t_run_ms += ms_since(t2);
   }
+  auto t3 = clk::now();
   pending_pops_.clear();
   max_live_buffers = std::max(max_live_buffers, live_buffer_count());
   compact(extra);
+  t_compact_ms += ms_since(t3);
 }
 
 int64_t Executor::live_buffer_count() const {

@@ -110,6 +110,11 @@ class Executor {
   int64_t max_live_buffers = 0;
   double compile_ms = 0.0;
   int64_t vm_launches = 0;
+  bool ran_as_vm_program = false;
+  // Host time split of flushes (ms): building segments, choosing the form,
+  // running them (launch + host work; device time overlaps), compacting.
+  // Printed to stderr at destruction when $BSZ_HOST_TIMES is set.
+  double t_segment_ms = 0, t_policy_ms = 0, t_run_ms = 0, t_compact_ms = 0;
   int64_t fused_launches() const;
   int64_t fused_fallbacks() const;
   void set_schedule(const Schedule& s);
@@ -201,6 +206,11 @@ class Executor {
   void compact(int* extra);
   void run_plain(const Segment& seg);
   void run_vm(const Segment& seg);
+  // Whole program, control flow included, as one device-interpreter launch
+  // (vmprog.cpp).  Returns false, with no state changed, when the program
+  // needs the host during its run (see vmprog.cpp for the conditions).
+  bool run_vm_program();
+  friend struct VmCompiler;
   bool fused_pays(const Segment& seg);
   const uint64_t* const_ptr(int node);
   void ensure_slots(int64_t need);

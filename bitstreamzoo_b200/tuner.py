@@ -79,6 +79,12 @@ def encode_schedule(s: dict) -> list[float]:
 
 
 N_SCHEDULE_FEATURES = 7
+N_PROGRAM_FEATURES = 14
+N_FEATURES = N_PROGRAM_FEATURES + 1 + N_SCHEDULE_FEATURES
+
+# The fitted model shipped with the package (written by
+# ``python -m bitstreamzoo_b200.tuner --out``).
+DEFAULT_MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "cost_model.npz")
 
 
 def program_features(prog) -> list[float]:
@@ -294,6 +300,16 @@ class CostModel:
         np.savez(path, params=self.params(), mu=self.mu, sd=self.sd, y=np.array([self.y_mu, self.y_sd]),
                  in_dim=np.array([self.in_dim]))
 
+    @classmethod
+    def load_default(cls, ctx, path: str | None = None):
+        """The shipped model, or None when it has not been trained."""
+        path = path or DEFAULT_MODEL_PATH
+        if not os.path.exists(path):
+            return None
+        m = cls(ctx, N_FEATURES)
+        m.load(path)
+        return m
+
     def load(self, path: str):
         z = np.load(path)
         assert int(z["in_dim"][0]) == self.in_dim
@@ -305,7 +321,7 @@ class CostModel:
 # ------------------------------------------------------------------- study --
 
 
-def tuning_suite(n_train: int = 24, n_test: int = 8, seed: int = 20261210, max_ops: int = 3000):
+def tuning_suite(n_train: int = 24, n_test: int = 8, seed: int = 20261210, max_ops: int = 1500):
     """Seeded training and held-out program sources.
 
     Each DAG draws its op mix from Dirichlet(1) over five classes (AND/OR/
