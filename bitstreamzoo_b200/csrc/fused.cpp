@@ -180,6 +180,10 @@ struct Gen {
   // subtree first, which keeps fewer values live inside a step than node-id
   // order (fewer registers, so more warps per SM).
   std::vector<int> emit_order;
+  // Small-shift sources: the last shift node (in emit_order) that reads
+  // them; that node also stores the carried edge bits for the next step, so
+  // no ballot result stays live across the step.
+  std::map<int, int> last_small_use;
   std::string pk(int bitpos) const { return "pk" + std::to_string(bitpos / 32); }
   std::vector<uint8_t> dyn;        // node dirt must be tracked during warm-up
   std::map<int, int64_t> sdh;      // static dirt (words) for nodes without add ancestors
@@ -292,6 +296,10 @@ struct Gen {
     }
     n_pack = (nb + 31) / 32;
     order_for_registers();
+    for (int n : emit_order) {
+      const Node& x = nodes[n];
+      if (x.op == NOp::Shl && x.a >= 0 && small_shl.count(x.a)) last_small_use[x.a] = n;
+    }
     make_slots();
   }
 
@@ -421,17 +429,30 @@ struct Gen {
             }
             s << "      }\n";
           } else if (small_shl.count(x.a)) {
-            const std::string cur = opnd(x.a), q = "q" + std::to_string(x.a);
+            // bits shifted in: bit 63 (and 62) of the word below, from one
+            // ballot per bit; lane 0 takes the previous step's lane 31 bits
+            const std::string cur = opnd(x.a);
             const int mb = mbit.at(x.a);
+            const bool last = last_small_use.at(x.a) == n;
+            const bool need62 = bs == 2 || (last && small_shl.at(x.a) == 2);
             const std::string w = pk(mb), sh = std::to_string(mb % 32), sh1 = std::to_string(mb % 32 + 1);
             s << "      u64 " << v(n) << ";\n      {\n"
-              << "        const u32 m63 = (" << q << "_63 << 1) | ((" << w << " >> " << sh << ") & 1u);\n";
+              << "        const u32 q63 = __ballot_sync(~0u, (" << cur << " >> 63) != 0ull);\n";
+            if (need62) s << "        const u32 q62 = __ballot_sync(~0u, ((" << cur << " >> 62) & 1ull) != 0ull);\n";
+            s << "        const u32 m63 = (q63 << 1) | ((" << w << " >> " << sh << ") & 1u);\n";
             if (bs == 1) {
               s << "        " << v(n) << " = (" << cur << " << 1) | (u64)((m63 >> lane) & 1u);\n";
             } else {
-              s << "        const u32 m62 = (" << q << "_62 << 1) | ((" << w << " >> " << sh1 << ") & 1u);\n"
+              s << "        const u32 m62 = (q62 << 1) | ((" << w << " >> " << sh1 << ") & 1u);\n"
                 << "        " << v(n) << " = (" << cur << " << 2) | (u64)(((m63 >> lane) & 1u) << 1) | "
                 << "(u64)((m62 >> lane) & 1u);\n";
+            }
+            if (last) {
+              const unsigned mask = small_shl.at(x.a) == 2 ? 3u : 1u;
+              s << "        " << w << " = (" << w << " & ~(" << mask << "u << " << sh << ")) | ((q63 >> 31) << " << sh
+                << ")";
+              if (small_shl.at(x.a) == 2) s << " | ((q62 >> 31) << " << sh1 << ")";
+              s << ";\n";
             }
             s << "      }\n";
           } else {
@@ -489,29 +510,11 @@ struct Gen {
           s << "      dh" << n << " = max(" << dh(x.a) << ", " << dh(x.b) << ");\n";
         }
       }
-      auto sm = small_shl.find(n);
-      if (sm != small_shl.end()) {
-        s << "      const u32 q" << n << "_63 = __ballot_sync(~0u, (" << v(n) << " >> 63) != 0ull);\n";
-        if (sm->second == 2)
-          s << "      const u32 q" << n << "_62 = __ballot_sync(~0u, ((" << v(n) << " >> 62) & 1ull) != 0ull);\n";
-      }
     }
-    // carry previous-step values of left-shifted temporaries (for 1-2 bit
-    // shifts only the last lane's top bits)
-    for (int n : shl_src) {
-      auto sm = small_shl.find(n);
-      if (sm == small_shl.end()) {
-        s << "      pv" << n << " = " << v(n) << ";\n";
-      } else {
-        const int mb = mbit.at(n);
-        const std::string w = pk(mb), sh = std::to_string(mb % 32);
-        const unsigned mask = sm->second == 2 ? 3u : 1u;
-        s << "      " << w << " = (" << w << " & ~(" << mask << "u << " << sh << ")) | ((q" << n << "_63 >> 31) << "
-          << sh << ")";
-        if (sm->second == 2) s << " | ((q" << n << "_62 >> 31) << " << (mb % 32 + 1) << ")";
-        s << ";\n";
-      }
-    }
+    // carry previous-step values of left-shifted temporaries (1-2 bit shift
+    // sources carry their edge bits at their last shift instead)
+    for (int n : shl_src)
+      if (!small_shl.count(n)) s << "      pv" << n << " = " << v(n) << ";\n";
     if (!track) {
       s << "      if (w < e) {\n";
       for (auto& kv : outs)
