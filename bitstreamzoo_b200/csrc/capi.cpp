@@ -419,6 +419,28 @@ int bsz_program_features(bsz_ctx* ctx, bsz_program* prog, float* out, int capaci
         default: break;
       }
     }
+    // peak number of simultaneously live computed values in node order (a
+    // proxy for the generated kernel's register demand per step)
+    std::vector<int64_t> last_use(nd.size(), -1);
+    for (size_t i = 0; i < nd.size(); ++i) {
+      if (!live[i]) continue;
+      for (int o : {nd[i].a, nd[i].b})
+        if (o >= 0) last_use[o] = static_cast<int64_t>(i);
+    }
+    for (int n : t.output_nodes)
+      if (n >= 0) last_use[n] = static_cast<int64_t>(nd.size());
+    for (auto& p : t.pops) last_use[p.first] = std::max<int64_t>(last_use[p.first], static_cast<int64_t>(nd.size()));
+    std::vector<int> ends(nd.size() + 1, 0);
+    int64_t cur = 0, peak = 0;
+    for (size_t i = 0; i < nd.size(); ++i) {
+      if (live[i] && !is_leaf(static_cast<int>(i)) && last_use[i] >= 0) {
+        ++cur;
+        peak = std::max(peak, cur);
+        ++ends[std::min<size_t>(static_cast<size_t>(last_use[i]), nd.size())];
+      }
+      cur -= ends[i];
+      ends[i] = 0;
+    }
     const double tot = std::max(1.0, n_ops);
     const float f[BSZ_NUM_FEATURES] = {
         static_cast<float>(std::log2(1 + n_ops)), static_cast<float>(n_bit / tot),
@@ -428,7 +450,8 @@ int bsz_program_features(bsz_ctx* ctx, bsz_program* prog, float* out, int capaci
         static_cast<float>(std::log2(1.0 + max_adepth)), static_cast<float>(std::log2(1 + max_ws)),
         static_cast<float>(std::log2(1 + n_in)),
         static_cast<float>(std::log2(1.0 + t.output_nodes.size() + t.pops.size())),
-        static_cast<float>(std::log2(1 + n_shl_t)), static_cast<float>(std::log2(1 + n_add))};
+        static_cast<float>(std::log2(1 + n_shl_t)), static_cast<float>(std::log2(1 + n_add)),
+        static_cast<float>(std::log2(1.0 + static_cast<double>(peak)))};
     for (int i = 0; i < BSZ_NUM_FEATURES && i < capacity; ++i) out[i] = f[i];
     count = BSZ_NUM_FEATURES;
   });

@@ -79,8 +79,8 @@ def encode_schedule(s: dict) -> list[float]:
 
 
 N_SCHEDULE_FEATURES = 7
-N_PROGRAM_FEATURES = 14
-N_FEATURES = N_PROGRAM_FEATURES + 1 + N_SCHEDULE_FEATURES
+N_PROGRAM_FEATURES = 15
+N_FEATURES = N_PROGRAM_FEATURES + 1 + N_SCHEDULE_FEATURES + 1
 
 # The fitted model shipped with the package (written by
 # ``python -m bitstreamzoo_b200.tuner --out``).
@@ -97,8 +97,18 @@ def program_features(prog) -> list[float]:
     return list(buf[:n])
 
 
+def register_pressure(pfeat: list[float], sched: dict) -> float:
+    """log2 of (registers the DAG's peak live values need, 2 per 64-bit value
+    plus ~16 of bookkeeping) over the register cap the schedule's launch
+    bounds allow: above 0 the generated kernel spills."""
+    peak = 2 ** pfeat[14] - 1
+    cap = min(255.0, 65536.0 / (32 * sched["warps"] * max(1, sched["min_blocks"])))
+    return math.log2(2 * peak + 16) - math.log2(cap)
+
+
 def feature_row(pfeat: list[float], nbits: int, sched: dict) -> list[float]:
-    return list(pfeat) + [math.log2(max(2, nbits))] + encode_schedule(sched)
+    return (list(pfeat) + [math.log2(max(2, nbits))] + encode_schedule(sched)
+            + [register_pressure(pfeat, sched)])
 
 
 # ------------------------------------------------------------- measurement --
@@ -366,8 +376,8 @@ def codegen_key(s: dict) -> tuple:
 
 
 def study(ctx, train_srcs, test_srcs, sizes=(1 << 23, 1 << 25, 1 << 27), candidates=None,
-          sample_frac: float = 0.25, reps: int = 3, steps: int = 3000, seed: int = 0, log=None,
-          weight_decay: float = 1e-4) -> dict:
+          sample_frac: float = 0.25, reps: int = 3, steps: int = 1500, seed: int = 0, log=None,
+          weight_decay: float = 0.02) -> dict:
     """Collects timings, fits a :class:`CostModel` and reports pick regret on
     the held-out programs for the model's top-1 and top-4 picks and for the
     default schedule.

@@ -166,7 +166,7 @@ void bsz_batch_free(bsz_batch* batch);
 /* DAG features of a straight-line program for the cost model (traced and
  * simplified as the fused form sees it): writes up to `capacity` floats,
  * returns the number of features (BSZ_NUM_FEATURES) or -1 on error. */
-#define BSZ_NUM_FEATURES 14
+#define BSZ_NUM_FEATURES 15
 int bsz_program_features(bsz_ctx* ctx, bsz_program* prog, float* out, int capacity);
 typedef struct bsz_mlp bsz_mlp;
 bsz_mlp* bsz_mlp_create(bsz_ctx* ctx, int in_dim, int hidden, int layers, uint64_t seed);

@@ -85,13 +85,14 @@ def test_program_features_of_a_known_program(ctx):
     src = ("input stream a\ninput stream b\noutput stream o\noutput int c\n"
            "stream t = a + b\no = t << 3\nc = popcount(o)\n")
     f = tuner.program_features(ctx.compile(src))
-    assert len(f) == 14
+    assert len(f) == 15
     assert f[0] == pytest.approx(math.log2(3))          # two ops
     assert f[5] == pytest.approx(0.5)                   # half are adds
     assert f[3] == pytest.approx(0.5)                   # half shift a temporary
     assert f[7] == pytest.approx(math.log2(3))          # depth 2
     assert f[8] == pytest.approx(1.0)                   # one add on the path
     assert f[10] == pytest.approx(math.log2(3))         # two inputs
+    assert f[14] == pytest.approx(math.log2(3))         # two values live at once
 
 
 def test_every_candidate_schedule_is_bit_exact(ctx):
