@@ -141,6 +141,17 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def reduce_max(x: float, dist, device) -> float:
+    """The maximum of x over all ranks (every rank gets it); x itself on one
+    rank.  Times are reported as the slowest rank's."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -311,11 +322,7 @@ def run_ours(args, rank, world, local):
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, dev)
 
     sched, sched_src = dict(bz.DEFAULT_SCHEDULE), "default"
     if args.schedule == "model":
@@ -536,10 +543,7 @@ def run_batched(args, rank, world, local):
     ck = clocks.stop()
     prof = ctx.profile_report()
     ctx.profile(False)
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_max(ms, dist, torch.device("cuda", local))
     # spot check: a few instances against their own single-program runs (fused form)
     rng = np.random.default_rng(rank)
     check = True
