@@ -299,137 +299,6 @@ k_add(uint64_t* __restrict__ d, const uint64_t* __restrict__ a, const uint64_t* 
   }
 }
 
-// Persistent, software-pipelined form of the same carry scan.  k_add runs
-// one tile per CTA, so each CTA's loads, look-back and stores happen in
-// sequence and the SM idles on memory between them; here a grid sized to the
-// resident-CTA limit loops over tiles taken in ticket order, and the loads of
-// its next tile are issued before the look-back and stores of the current
-// one, so every CTA keeps a tile of loads in flight at all times.  Each CTA
-// publishes its tile's aggregate before it waits, and waits only on lower
-// tiles, so the look-back cannot deadlock.  Same state layout and results as
-// k_add.
-__global__ void __launch_bounds__(kAddWarps * 32)
-k_add_persistent(uint64_t* __restrict__ d, const uint64_t* __restrict__ a, const uint64_t* __restrict__ b,
-                 int64_t n, uint64_t last_mask, uint32_t* __restrict__ state, uint32_t* __restrict__ err,
-                 int64_t n_tiles) {
-  __shared__ uint32_t s_tile[2];
-  __shared__ uint32_t s_wagg[kAddWarps];
-  __shared__ uint32_t s_cin;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t* status = state + 1;
-  if (threadIdx.x == 0) s_tile[0] = atomicAdd(&state[0], 1u);
-  __syncthreads();
-  int64_t tile = s_tile[0];
-  int buf = 0;
-  uint64_t x[kAddSteps], y[kAddSteps];
-  {
-    const int64_t wb = tile * kAddTile + static_cast<int64_t>(warp) * kAddSteps * 32 + lane;
-#pragma unroll
-    for (int j = 0; j < kAddSteps; ++j) {
-      const int64_t w = wb + j * 32;
-      x[j] = (tile < n_tiles && w < n) ? a[w] : 0;
-      y[j] = (tile < n_tiles && w < n) ? b[w] : 0;
-    }
-  }
-  while (tile < n_tiles) {
-    // next ticket (the other smem slot: the current one may still be read)
-    if (threadIdx.x == 0) s_tile[buf ^ 1] = atomicAdd(&state[0], 1u);
-    const int64_t wbase = tile * kAddTile + static_cast<int64_t>(warp) * kAddSteps * 32 + lane;
-    uint32_t G[kAddSteps], P[kAddSteps];
-#pragma unroll
-    for (int j = 0; j < kAddSteps; ++j) {
-      const int64_t w = wbase + j * 32;
-      const uint64_t s = x[j] + y[j];
-      G[j] = __ballot_sync(0xffffffffu, s < x[j]);
-      P[j] = __ballot_sync(0xffffffffu, w < n && s == ~uint64_t(0));
-      x[j] = s;
-    }
-    __syncthreads();   // s_tile[buf ^ 1] visible; s_wagg / s_cin free from the last tile
-    const int64_t next = s_tile[buf ^ 1];
-    // issue the next tile's loads now; they land while this tile resolves
-    uint64_t nx[kAddSteps];
-    {
-      const int64_t wb = next * kAddTile + static_cast<int64_t>(warp) * kAddSteps * 32 + lane;
-#pragma unroll
-      for (int j = 0; j < kAddSteps; ++j) {
-        const int64_t w = wb + j * 32;
-        nx[j] = (next < n_tiles && w < n) ? a[w] : 0;
-        y[j] = (next < n_tiles && w < n) ? b[w] : 0;
-      }
-    }
-    uint32_t wg = 0, wp = 1;
-#pragma unroll
-    for (int j = 0; j < kAddSteps; ++j) {
-      const uint64_t z = static_cast<uint64_t>(G[j] | P[j]) + G[j];
-      const uint32_t sg = static_cast<uint32_t>(z >> 32);
-      const uint32_t sp = P[j] == 0xffffffffu;
-      wg = sg | (sp & wg);
-      wp &= sp;
-    }
-    if (lane == 0) s_wagg[warp] = wg | (wp << 1);
-    __syncthreads();
-    if (warp == 0) {
-      uint32_t tg = 0, tp = 1;
-#pragma unroll
-      for (int v = 0; v < kAddWarps; ++v) {
-        const uint32_t g = s_wagg[v] & 1u, p = s_wagg[v] >> 1;
-        tg = g | (p & tg);
-        tp &= p;
-      }
-      uint32_t cin = 0;
-      if (lane == 0) {
-        if (tile == 0) {
-          st_volatile(&status[0], kFlagInc | tg);
-        } else {
-          st_volatile(&status[tile], kFlagAgg | tg | (tp << 1));
-          uint32_t ag = 0, ap = 1;
-          int64_t j = tile - 1;
-          int spins = 0;
-          while (true) {
-            const uint32_t v = ld_volatile(&status[j]);
-            const uint32_t f = v & kFlagMask;
-            if (f == 0) {
-              if (++spins > kSpinLimit) { atomicOr(err, kErrLookbackTimeout); cin = 0; break; }
-              __nanosleep(32);
-              continue;
-            }
-            if (f == kFlagInc) { cin = ag | (ap & (v & 1u)); break; }
-            ag = ag | (ap & (v & 1u));
-            ap &= (v >> 1) & 1u;
-            if (!ap) { cin = ag; break; }
-            --j;
-            spins = 0;
-          }
-          __threadfence();
-          st_volatile(&status[tile], kFlagInc | (tg | (tp & cin)));
-        }
-        s_cin = cin;
-      }
-    }
-    __syncthreads();
-    uint32_t c = s_cin;
-    for (int v = 0; v < warp; ++v) {
-      const uint32_t g = s_wagg[v] & 1u, p = s_wagg[v] >> 1;
-      c = g | (p & c);
-    }
-#pragma unroll
-    for (int j = 0; j < kAddSteps; ++j) {
-      const uint64_t z = static_cast<uint64_t>(G[j] | P[j]) + G[j] + c;
-      const uint32_t carries = static_cast<uint32_t>(z) ^ P[j];
-      c = static_cast<uint32_t>(z >> 32);
-      const int64_t w = wbase + j * 32;
-      if (w < n) {
-        uint64_t r = x[j] + ((carries >> lane) & 1u);
-        if (w == n - 1) r &= last_mask;
-        d[w] = r;
-      }
-      x[j] = nx[j];
-    }
-    tile = next;
-    buf ^= 1;
-  }
-}
-
 // ---- reductions ------------------------------------------------------------
 __device__ __forceinline__ uint64_t warp_sum(uint64_t v) {
 #pragma unroll
@@ -536,20 +405,9 @@ void launch_add_with_state(Device& dev, uint64_t* d, const uint64_t* a, const ui
   if (n <= 0) return;
   int64_t tiles = (n + kAddTile - 1) / kAddTile;
   if (tiles > 0x7fffffff) throw std::invalid_argument("launch_add: stream too long");
-  // resident CTAs per SM of the persistent kernel (computed once per process)
-  static int per_sm = [] {
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_add_persistent, kAddWarps * 32, 0) != cudaSuccess ||
-        b < 1) {
-      cudaGetLastError();
-      b = 1;
-    }
-    return b;
-  }();
-  const int64_t grid = std::min<int64_t>(tiles, static_cast<int64_t>(dev.sm_count()) * per_sm);
   ProfScope prof(dev, "k_add");
-  k_add_persistent<<<static_cast<unsigned>(grid), kAddWarps * 32, 0, dev.stream()>>>(
-      d, a, b, n, last_mask, state, dev.error_word(), tiles);
+  k_add<<<static_cast<unsigned>(tiles), kAddWarps * 32, 0, dev.stream()>>>(
+      d, a, b, n, last_mask, state, dev.error_word());
   check_launch();
   ++dev.n_launches;
 }
