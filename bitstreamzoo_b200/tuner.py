@@ -428,6 +428,7 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 23, 1 << 25, 1 << 27), candida
 
     default_key = schedule_key(DEFAULT_SCHEDULE)
     rows = []
+    raw_test = []
     for i, src in enumerate(test_srcs):
         prog, pf = prog_of(src)
         for n in sizes:
@@ -435,6 +436,10 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 23, 1 << 25, 1 << 27), candida
                      for s in candidates}
             if default_key not in times:
                 times[default_key] = measure(ctx, prog, n, bufs_by_size[n][1], DEFAULT_SCHEDULE, reps=reps)
+            raw_test.append({"program": i, "bits": n,
+                             "X": [feature_row(pf, n, s) for s in candidates],
+                             "ms": [times[schedule_key(s)] for s in candidates],
+                             "default_ms": times[default_key]})
             ranked = model.rank(pf, n, candidates)
             top4 = min(times[schedule_key(s)] for s in ranked[:4])
             best = min(times.values())
@@ -456,7 +461,9 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 23, 1 << 25, 1 << 27), candida
             "loss_last": float(np.mean(losses[-20:])), "collect_s": t_collect, "fit_s": t_fit,
             "regret_top1": stats("regret_top1"), "regret_top4": stats("regret_top4"),
             "regret_default": stats("regret_default"),
-            "exhaustive_timings_per_case": len(candidates)}
+            "exhaustive_timings_per_case": len(candidates),
+            # every timing, for offline study of the model
+            "raw": {"train_X": X, "train_ms": y, "train_groups": groups, "test": raw_test}}
 
 
 def main(argv=None):
@@ -481,7 +488,7 @@ def main(argv=None):
     model = rep.pop("model")
     if a.out:
         model.save(a.out)
-    summary = {k: v for k, v in rep.items() if k != "rows"}
+    summary = {k: v for k, v in rep.items() if k not in ("rows", "raw")}
     print(json.dumps(summary))
     if a.json:
         with open(a.json, "w") as f:
