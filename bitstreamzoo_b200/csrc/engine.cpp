@@ -530,7 +530,7 @@ void Executor::flush(const Bits* live, int* extra) {
     if (vm) {
       run_vm(seg);
     } else if (fuse) {
-      for (int i : seg.inputs) const_ptr(i);
+      // constants need no buffer: the generated code computes their words
       fused_->run(nodes_, seg, N_, nw_, d_slots_, &compile_ms);
     } else {
       run_plain(seg);

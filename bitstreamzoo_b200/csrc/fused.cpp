@@ -1148,9 +1148,13 @@ BatchRunner::BatchRunner(Device& dev, const std::vector<const Program*>& progs,
     a[m.max_in + m.max_out + 3] = static_cast<uint64_t>(range);
     a[m.max_in + m.max_out + 4] = mask_for_bits(bi.bitlength > 0 ? bi.bitlength : 64 * nw);
   }
-  // longest items first: the atomic work queue then balances the tail
-  std::stable_sort(items.begin(), items.end(),
-                   [](const BatchItem& x, const BatchItem& y) { return (x.e - x.s) > (y.e - y.s); });
+  // items of one program together (warps then run the same device function,
+  // so the instruction cache holds one DAG at a time), longest first within
+  // it so the atomic work queue balances the tail
+  std::stable_sort(items.begin(), items.end(), [](const BatchItem& x, const BatchItem& y) {
+    if (x.dag != y.dag) return x.dag < y.dag;
+    return (x.e - x.s) > (y.e - y.s);
+  });
   m.n_items = static_cast<int64_t>(items.size());
   BSZ_CUDA(cudaMalloc(&m.d_slots, static_cast<size_t>(std::max<int64_t>(m.n_slots, 1)) * 8));
   ++dev.n_mallocs;
