@@ -158,3 +158,12 @@ def test_tuning_study_end_to_end(ctx):
         assert math.isfinite(r["best_ms"]) and r["best_ms"] > 0
     choice = rep["model"].choose(ctx.compile(test[0]), 1 << 23, cands)
     assert tuner.schedule_key(choice) in {tuner.schedule_key(s) for s in cands}
+
+
+def test_shipped_cost_model_picks_from_the_space(ctx):
+    m = tuner.CostModel.load_default(ctx)
+    assert m is not None, "bitstreamzoo_b200/data/cost_model.npz is missing"
+    prog = ctx.compile(regex_dag_src(n_ops=300, seed=5))
+    keys = {tuner.schedule_key(s) for s in tuner.CANDIDATES}
+    for nbits in (1 << 20, 1 << 26):
+        assert tuner.schedule_key(m.choose(prog, nbits)) in keys
