@@ -566,9 +566,11 @@ struct Gen {
   std::string device_function(const std::string& name) {
     analyze();
     std::ostringstream s;
+    // the instance's argument block stays in global memory (read-only,
+    // not aliased): copying it would pin ~20 registers for the whole item
     s << "__device__ __noinline__ void " << name
-      << "(const Args& Ap, const long long s, const long long e, const int lane) {\n"
-      << "  const Args A = Ap;\n";
+      << "(const Args* __restrict__ Ap, const long long s, const long long e, const int lane) {\n"
+      << "  const Args& A = *Ap;\n";
     body(s);
     s << "}\n";
     return s.str();
@@ -1117,7 +1119,7 @@ BatchRunner::BatchRunner(Device& dev, const std::vector<const Program*>& progs,
       << "    const Item I = items[it];\n"
       << "    switch (I.dag) {\n";
   for (size_t k = 0; k < m.progs.size(); ++k)
-    src << "      case " << k << ": dag_" << k << "(insts[I.inst], I.s, I.e, lane); break;\n";
+    src << "      case " << k << ": dag_" << k << "(insts + I.inst, I.s, I.e, lane); break;\n";
   src << "      default: break;\n    }\n  }\n}\n";
   m.kern = compile_source(src.str(), sched.warps * 32, &compile_ms, "bsz_batch");
   // 3. argument blocks (one Args per instance), slots and work items
