@@ -236,26 +236,34 @@ def cpu_baseline(workload: str, nbits: int, reps: int, warm: int = 1):
             write_bsdata(data, nbits, w.inputs)
             env = dict(os.environ, OMP_NUM_THREADS=str(threads),
                        GLIBC_TUNABLES="glibc.cpu.x86_rep_stosb_threshold=2000000000")
-            times = []
-            for i in range(warm + reps):
-                out = os.path.join(td, "out.json")
-                with open(out, "w") as fo:
-                    r = subprocess.run([bsim, prog, "--backend", "simd_omp", "--reuse-mem",
-                                        "--input", data], stdout=fo, stderr=subprocess.PIPE,
-                                       env=env, timeout=900)
-                if r.returncode != 0:
-                    raise RuntimeError(r.stderr.decode()[-500:])
-                with open(out, "rb") as fi:
-                    head = fi.read(4096).decode(errors="replace")
-                ms = float(head.split('"exec_ms":', 1)[1].split(",", 1)[0])
-                if i >= warm:
-                    times.append(ms)
-        ms = statistics.median(times)
+
+            def run_bsim(backend, n_runs, n_warm):
+                times = []
+                for i in range(n_warm + n_runs):
+                    out = os.path.join(td, "out.json")
+                    with open(out, "w") as fo:
+                        r = subprocess.run([bsim, prog, "--backend", backend, "--reuse-mem",
+                                            "--input", data], stdout=fo, stderr=subprocess.PIPE,
+                                           env=env, timeout=900)
+                    if r.returncode != 0:
+                        raise RuntimeError(r.stderr.decode()[-500:])
+                    with open(out, "rb") as fi:
+                        head = fi.read(4096).decode(errors="replace")
+                    t = float(head.split('"exec_ms":', 1)[1].split(",", 1)[0])
+                    if i >= n_warm:
+                        times.append(t)
+                return statistics.median(times)
+
+            ms = run_bsim("simd_omp", reps, warm)
+            # the reference's single-core AVX-512 form, once, beside it
+            ms1 = run_bsim("simd", 1, 0)
         return {"value": w.in_bytes / (ms * 1e-3) / 1e9, "unit": "GB/s", "cores": threads,
+                "single_core": {"value": w.in_bytes / (ms1 * 1e-3) / 1e9, "unit": "GB/s", "cores": 1,
+                                "backend": "bsim --backend simd", "ms": ms1},
                 "kind": "reference", "ms_per_step": ms,
                 "sample": (f"{workload} program at {nbits} bits per stream (1/{max(1, full // nbits)} "
                            f"of the {full}-bit workload), bsim --backend simd_omp, "
-                           f"OMP_NUM_THREADS={threads}, median exec_ms of {len(times)} runs")}
+                           f"OMP_NUM_THREADS={threads}, median exec_ms of {reps} runs")}
     from oracle import cwords, pyoracle
     prog = pyoracle.parse(w.src)
     times = []
