@@ -217,9 +217,29 @@ int Executor::mk(NOp op, int a, int b, int64_t k) {
 
 // ------------------------------------------------------------------ walk ---
 
+// Per-class counters on the walk's hot path; op_mix (keyed by the
+// reference's op names) is filled from them when the run ends.
 void Executor::count(const char* op) {
   ++op_count;
-  ++op_mix[op];
+  int k;
+  switch (op[0]) {
+    case '~': k = 0; break;
+    case '&': k = 1; break;
+    case '|': k = 2; break;
+    case '^': k = 3; break;
+    case '+': k = 4; break;
+    case '<': k = 5; break;
+    case '>': k = 6; break;
+    default: k = 7; break;   // popcount
+  }
+  ++op_class_[k];
+}
+
+void Executor::publish_op_mix() {
+  static const char* const kNames[8] = {"~", "&", "|", "^", "+", "<<", ">>", "popcount"};
+  for (int k = 0; k < 8; ++k)
+    if (op_class_[k]) op_mix[kNames[k]] += op_class_[k];
+  for (auto& c : op_class_) c = 0;
 }
 
 int Executor::read_var(int name) {
@@ -447,6 +467,7 @@ void Executor::run() {
   exec_block(prog_.stmts);
   flush(&live_end_, nullptr);
   resolve_slots();
+  publish_op_mix();
   // Outputs bound to constants get a buffer so the caller can read them.
   auto materialize = [&](int& node) {
     Node& n = nodes_[node];

@@ -196,6 +196,8 @@ class Executor {
   bool nonzero(int node, const Stmt* at);
   IntV popcount(int node);
   void count(const char* op);
+  void publish_op_mix();
+  int64_t op_class_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
   // graph
   int mk(NOp op, int a = -1, int b = -1, int64_t k = 0);
