@@ -56,8 +56,8 @@ Executor::Executor(Device& dev, const Program& prog, int64_t bitlength, ExecOpti
   if (opt_.mode != ExecMode::Plain) opt_.simplify = true;
   if (opt_.mode == ExecMode::Fused || opt_.mode == ExecMode::Auto)
     fused_ = std::make_unique<FusedBackend>(dev_, opt_);
-  BSZ_CUDA(cudaMalloc(&d_flag_, 256));
-  ++dev_.n_mallocs;
+  flag_buf_ = dev_.alloc_stream(32);
+  d_flag_ = reinterpret_cast<unsigned int*>(flag_buf_->p);
   compute_liveness();
 }
 
@@ -70,9 +70,7 @@ Executor::~Executor() {
                  static_cast<long long>(fused_launches()), static_cast<long long>(op_count), t_segment_ms,
                  t_policy_ms, t_run_ms, t_compact_ms, compile_ms);
   cudaStreamSynchronize(dev_.stream());
-  if (d_flag_) cudaFree(d_flag_);
-  if (d_slots_) cudaFree(d_slots_);
-  if (vm_buf_) cudaFree(vm_buf_);
+  // flag, slot and VM buffers go back to the device's cache with their BufRefs
 }
 
 void Executor::set_schedule(const Schedule& s) {
@@ -740,14 +738,11 @@ void Executor::run_vm(const Segment& seg) {
   const size_t file_b = smem ? 0 : static_cast<size_t>(n_slots) * static_cast<size_t>(nw_) * 8;
   const size_t total = align(ops_b) + align(ext_b) + file_b;
   if (total > vm_cap_) {
-    if (vm_buf_) {
-      BSZ_CUDA(cudaStreamSynchronize(dev_.stream()));
-      BSZ_CUDA(cudaFree(vm_buf_));
-      vm_buf_ = nullptr;
-    }
+    // the old block returns to the device cache; stream order keeps it
+    // alive for work already queued on it
     vm_cap_ = std::max<size_t>(total, size_t(1) << 20);
-    BSZ_CUDA(cudaMalloc(&vm_buf_, vm_cap_));
-    ++dev_.n_mallocs;
+    vm_mem_ = dev_.alloc_stream(static_cast<int64_t>((vm_cap_ + 7) / 8));
+    vm_buf_ = vm_mem_->p;
   }
   char* base = static_cast<char*>(vm_buf_);
   VmOp* d_ops = reinterpret_cast<VmOp*>(base);
@@ -799,8 +794,8 @@ void Executor::compact(int* extra) {
 void Executor::ensure_slots(int64_t need) {
   if (slot_cap_ == 0) {
     slot_cap_ = kSlotChunk;
-    BSZ_CUDA(cudaMalloc(&d_slots_, static_cast<size_t>(slot_cap_) * 8));
-    ++dev_.n_mallocs;
+    slots_buf_ = dev_.alloc_stream(slot_cap_);
+    d_slots_ = reinterpret_cast<unsigned long long*>(slots_buf_->p);
     BSZ_CUDA(cudaMemsetAsync(d_slots_, 0, static_cast<size_t>(slot_cap_) * 8, dev_.stream()));
   }
   if (n_slots_ - slot_base_ + need > slot_cap_) {

@@ -167,6 +167,9 @@ class Executor {
 
   // popcount slots
   unsigned long long* d_slots_ = nullptr;
+  BufRef slots_buf_;              // device buffers below come from the device's buffer
+  BufRef flag_buf_;               // cache, so a run makes no cudaMalloc/cudaFree (each
+  BufRef vm_mem_;                 // cudaFree would synchronize the whole device)
   int64_t slot_cap_ = 0, slot_base_ = 0, n_slots_ = 0;
   std::vector<uint64_t> slot_val_;
   std::vector<std::pair<int, int64_t>> pending_pops_;

@@ -115,13 +115,11 @@ bool is_const(NOp op) { return op == NOp::Zero || op == NOp::OnesMask || op == N
 struct FusedBackend::Impl {
   Device& dev;
   ExecOptions opt;
+  BufRef fail_buf;   // from the device's buffer cache: no cudaMalloc/cudaFree per run
   unsigned int* d_fail = nullptr;
   Impl(Device& d, const ExecOptions& o) : dev(d), opt(o) {
-    BSZ_CUDA(cudaMalloc(&d_fail, 256));
-    ++dev.n_mallocs;
-  }
-  ~Impl() {
-    if (d_fail) cudaFree(d_fail);
+    fail_buf = dev.alloc_stream(32);
+    d_fail = reinterpret_cast<unsigned int*>(fail_buf->p);
   }
 };
 

@@ -474,14 +474,11 @@ bool Executor::run_vm_program() {
   const size_t file_b = smem ? 0 : static_cast<size_t>(c.n_slots) * static_cast<size_t>(nw_) * 8;
   const size_t total = align(ops_b) + align(ext_b) + align(state_b) + file_b;
   if (total > vm_cap_) {
-    if (vm_buf_) {
-      BSZ_CUDA(cudaStreamSynchronize(dev_.stream()));
-      BSZ_CUDA(cudaFree(vm_buf_));
-      vm_buf_ = nullptr;
-    }
+    // the old block returns to the device cache; stream order keeps it
+    // alive for work already queued on it
     vm_cap_ = std::max<size_t>(total, size_t(1) << 20);
-    BSZ_CUDA(cudaMalloc(&vm_buf_, vm_cap_));
-    ++dev_.n_mallocs;
+    vm_mem_ = dev_.alloc_stream(static_cast<int64_t>((vm_cap_ + 7) / 8));
+    vm_buf_ = vm_mem_->p;
   }
   char* base = static_cast<char*>(vm_buf_);
   VmOp* d_ops = reinterpret_cast<VmOp*>(base);
