@@ -281,17 +281,13 @@ int bsz_execute(bsz_run* run, bsz_stats* stats) {
     bsz::Device& dev = *run->prog->ctx->dev;
     bsz::Executor& ex = executor(run);
     const int64_t l0 = dev.n_launches;
-    cudaEvent_t e0, e1;
-    BSZ_CUDA(cudaEventCreate(&e0));
-    BSZ_CUDA(cudaEventCreate(&e1));
+    cudaEvent_t e0 = dev.exec_event(0), e1 = dev.exec_event(1);
     BSZ_CUDA(cudaEventRecord(e0, dev.stream()));
     ex.run();
     BSZ_CUDA(cudaEventRecord(e1, dev.stream()));
     BSZ_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     run->done = true;
     if (stats) {
       stats->op_count = ex.op_count;

@@ -76,6 +76,9 @@ class Device {
   int64_t bytes_live = 0;
   int64_t bytes_peak = 0;
 
+  // Two timing events reused by every execution on this device.
+  cudaEvent_t exec_event(int i);
+
   // Untyped device scratch (cached; grows).
   void* scratch(size_t bytes);
 
@@ -109,6 +112,7 @@ class Device {
   size_t scratch_cap_ = 0;
   void* pin_[2] = {nullptr, nullptr};
   cudaEvent_t pin_ev_[2] = {nullptr, nullptr};
+  cudaEvent_t exec_ev_[2] = {nullptr, nullptr};
   void ensure_pinned();
   void* raw_alloc(size_t bytes);
   struct ProfRec { const char* name; cudaEvent_t a, b; };

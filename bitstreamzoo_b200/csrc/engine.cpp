@@ -530,6 +530,16 @@ void Executor::flush(const Bits* live, int* extra) {
     else seg.inputs.push_back(i);
   }
   for (auto& p : pending_pops_) seg.pops.push_back({p.first, p.second - slot_base_});
+  if (!seg.pops.empty()) {
+    // this segment's popcount slots (allocated consecutively since the last
+    // flush) start at zero: the kernels accumulate into them
+    int64_t lo = seg.pops.front().second, hi = lo;
+    for (auto& p : seg.pops) {
+      lo = std::min(lo, p.second);
+      hi = std::max(hi, p.second);
+    }
+    BSZ_CUDA(cudaMemsetAsync(d_slots_ + lo, 0, static_cast<size_t>(hi - lo + 1) * 8, dev_.stream()));
+  }
   t_segment_ms += ms_since(t0);
   if (!seg.order.empty() || !seg.pops.empty()) {
     ++n_segments;
@@ -796,13 +806,12 @@ void Executor::ensure_slots(int64_t need) {
     slot_cap_ = kSlotChunk;
     slots_buf_ = dev_.alloc_stream(slot_cap_);
     d_slots_ = reinterpret_cast<unsigned long long*>(slots_buf_->p);
-    BSZ_CUDA(cudaMemsetAsync(d_slots_, 0, static_cast<size_t>(slot_cap_) * 8, dev_.stream()));
   }
   if (n_slots_ - slot_base_ + need > slot_cap_) {
     resolve_slots();
-    BSZ_CUDA(cudaMemsetAsync(d_slots_, 0, static_cast<size_t>(slot_cap_) * 8, dev_.stream()));
     slot_base_ = n_slots_;
   }
+  // (the slots a segment accumulates into are zeroed when it runs: flush())
   if (static_cast<int64_t>(slot_val_.size()) < n_slots_ + need) slot_val_.resize(n_slots_ + need + 1024);
 }
 
