@@ -41,6 +41,7 @@
 #include <mutex>
 #include <set>
 #include <sstream>
+#include <unordered_map>
 
 namespace bsz {
 namespace {
@@ -836,17 +837,69 @@ std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg, bool
 
 }  // namespace
 
+namespace {
+
+// Generating a part's source costs tens of microseconds per run; a compact
+// key of everything the generator reads (the part's nodes, its inputs'
+// kinds and tails, outputs, popcount slots, masking and schedule) maps a
+// repeated part straight to its compiled kernel and warm-up length.
+struct PartKernel {
+  Compiled c;
+  int64_t warm = 0;
+};
+std::mutex g_part_mu;
+std::unordered_map<std::string, PartKernel>& part_cache() {
+  static std::unordered_map<std::string, PartKernel> m;
+  return m;
+}
+
+std::string part_key(const std::vector<Node>& nodes, const Part& p, bool masked, const Schedule& sc) {
+  std::string k;
+  auto put = [&](int64_t v) { k.append(reinterpret_cast<const char*>(&v), sizeof v); };
+  auto node = [&](int n) {
+    const Node& x = nodes[n];
+    put(n);
+    put(static_cast<int64_t>(x.op) | (static_cast<int64_t>(x.tail) << 8) | (static_cast<int64_t>(x.clean) << 16));
+    put(x.a);
+    put(x.b);
+    put(x.k);
+  };
+  put(static_cast<int64_t>(p.order.size()));
+  for (int n : p.order) node(n);
+  put(static_cast<int64_t>(p.inputs.size()));
+  for (int n : p.inputs) node(n);
+  put(static_cast<int64_t>(p.outputs.size()));
+  for (int n : p.outputs) put(n);
+  put(static_cast<int64_t>(p.pops.size()));
+  for (auto& q : p.pops) {
+    put(q.first);
+    put(q.second);
+  }
+  put(masked);
+  put(sc.warps);
+  put(sc.min_blocks);
+  put(sc.prefetch);
+  return k;
+}
+
+}  // namespace
+
 bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& seg, int64_t N) {
   const Schedule& sc = impl_->opt.sched;
   std::vector<Part> parts = split(nodes, seg, sc.cut_adds != 0);
   for (Part& p : parts) {
     if (p.order.empty() && p.pops.empty()) continue;
     if (p.inputs.size() > kMaxInputs) return false;
+    {
+      std::lock_guard<std::mutex> lk(g_part_mu);
+      if (part_cache().count(part_key(nodes, p, (N % 64) != 0, sc))) continue;
+    }
     Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
     if (!is_compiled(g.source())) return false;
   }
   return true;
 }
+
 
 void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, int64_t nw,
                        unsigned long long* d_slots, double* compile_ms) {
@@ -857,9 +910,26 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
   for (Part& p : parts) {
     if (p.order.empty() && p.pops.empty()) continue;
     if (p.inputs.size() > kMaxInputs) throw RuntimeError("fused: too many inputs in one segment");
-    Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
-    const std::string src = g.source();
-    Compiled c = compile_source(src, sc.warps * 32, compile_ms);
+    const std::string key = part_key(nodes, p, (N % 64) != 0, sc);
+    PartKernel pk;
+    bool hit = false;
+    {
+      std::lock_guard<std::mutex> lk(g_part_mu);
+      auto it = part_cache().find(key);
+      if (it != part_cache().end()) {
+        pk = it->second;
+        hit = true;
+      }
+    }
+    if (!hit) {
+      Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
+      const std::string src = g.source();
+      pk.c = compile_source(src, sc.warps * 32, compile_ms);
+      pk.warm = g.warm;
+      std::lock_guard<std::mutex> lk(g_part_mu);
+      part_cache()[key] = pk;
+    }
+    const Compiled& c = pk.c;
     // outputs
     for (int n : p.outputs)
       if (!nodes[n].buf) nodes[n].buf = dev.alloc_stream(nw);
@@ -877,7 +947,7 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
     // persistent grid: as many warps as the compiled kernel keeps resident
     const int per_sm = sc.ctas_per_sm > 0 ? std::min(sc.ctas_per_sm, c.blocks_per_sm) : c.blocks_per_sm;
     int64_t max_warps = static_cast<int64_t>(dev.sm_count()) * per_sm * sc.warps;
-    int64_t min_range_steps = std::max<int64_t>(sc.range_steps, (g.warm / 32) * 8);
+    int64_t min_range_steps = std::max<int64_t>(sc.range_steps, (pk.warm / 32) * 8);
     int64_t warps_needed = std::max<int64_t>(1, std::min(max_warps, (steps + min_range_steps - 1) / min_range_steps));
     int64_t range = ((steps + warps_needed - 1) / warps_needed) * 32;
     int64_t total_warps = (nw + range - 1) / range;
