@@ -23,7 +23,8 @@ class Stats(ctypes.Structure):
                 ("n_syncs", ctypes.c_int64), ("peak_bytes", ctypes.c_int64),
                 ("max_live", ctypes.c_int64), ("kernel_ms", ctypes.c_double),
                 ("compile_ms", ctypes.c_double), ("n_fused_launches", ctypes.c_int64),
-                ("n_fused_fallbacks", ctypes.c_int64), ("n_vm_launches", ctypes.c_int64)]
+                ("n_fused_fallbacks", ctypes.c_int64), ("n_vm_launches", ctypes.c_int64),
+                ("walk_replayed", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

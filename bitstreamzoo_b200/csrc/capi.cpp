@@ -302,6 +302,7 @@ int bsz_execute(bsz_run* run, bsz_stats* stats) {
       stats->n_fused_launches = ex.fused_launches();
       stats->n_fused_fallbacks = ex.fused_fallbacks();
       stats->n_vm_launches = ex.vm_launches;
+      stats->walk_replayed = ex.walk_replayed ? 1 : 0;
     }
   });
 }

@@ -35,7 +35,106 @@ bool commutative(NOp op) {
   return op == NOp::And || op == NOp::Or || op == NOp::Xor || op == NOp::Add;
 }
 
+template <class T>
+void put_raw(std::string& s, T v) {
+  s.append(reinterpret_cast<const char*>(&v), sizeof v);
+}
+
+// At most this many cached walks per program (oldest evicted first).
+constexpr size_t kMaxWalks = 16;
+
 }  // namespace
+
+// A straight-line walk: everything run() reads after exec_block() and before
+// the final flush.  Nodes below n0 (the constants and the bound inputs, the
+// same ids for the same bindings) are not stored; the stored ones have no
+// buffers.
+struct Executor::WalkSnap {
+  size_t n0 = 0;
+  std::vector<Node> nodes;
+  std::vector<int> var;
+  std::vector<IntV> ints;
+  std::vector<uint8_t> int_def;
+  std::vector<std::unique_ptr<Arr>> arrs;
+  std::vector<IE> iexpr;
+  std::vector<std::pair<int, int64_t>> pops;
+  int64_t n_slots = 0;
+  int64_t op_count = 0;
+  int64_t op_class[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+struct Executor::ExecCache {
+  std::shared_ptr<const Liveness> live;
+  std::unordered_map<std::string, std::shared_ptr<const WalkSnap>> walks;
+  std::vector<std::string> order;   // insertion order, for eviction
+};
+
+Executor::ExecCache& Executor::exec_cache() const {
+  std::lock_guard<std::mutex> lk(prog_.exec_mu);
+  if (!prog_.exec_cache) prog_.exec_cache = std::make_shared<ExecCache>();
+  return *static_cast<ExecCache*>(prog_.exec_cache.get());
+}
+
+std::string Executor::walk_key() const {
+  std::string k = bind_sig_;
+  put_raw(k, N_);
+  put_raw(k, static_cast<int>(opt_.mode));
+  put_raw(k, opt_.simplify);
+  return k;
+}
+
+bool Executor::replay_walk(const std::string& key) {
+  std::shared_ptr<const WalkSnap> s;
+  {
+    ExecCache& c = exec_cache();
+    std::lock_guard<std::mutex> lk(prog_.exec_mu);
+    auto it = c.walks.find(key);
+    if (it == c.walks.end()) return false;
+    s = it->second;
+  }
+  if (nodes_.size() != s->n0 || n_slots_ != 0 || !pending_pops_.empty()) return false;
+  nodes_.insert(nodes_.end(), s->nodes.begin(), s->nodes.end());
+  var_ = s->var;
+  ints_ = s->ints;
+  int_def_ = s->int_def;
+  for (size_t i = 0; i < arrs_.size(); ++i)
+    arrs_[i] = s->arrs[i] ? std::make_unique<Arr>(*s->arrs[i]) : nullptr;
+  iexpr_ = s->iexpr;
+  if (s->n_slots > 0) ensure_slots(s->n_slots);
+  n_slots_ = s->n_slots;
+  pending_pops_ = s->pops;
+  op_count = s->op_count;
+  for (int k = 0; k < 8; ++k) op_class_[k] = s->op_class[k];
+  return true;
+}
+
+void Executor::save_walk(const std::string& key, size_t n0) {
+  for (size_t i = n0; i < nodes_.size(); ++i)
+    if (nodes_[i].buf) return;   // not a pure walk
+  auto s = std::make_shared<WalkSnap>();
+  s->n0 = n0;
+  s->nodes.assign(nodes_.begin() + static_cast<std::ptrdiff_t>(n0), nodes_.end());
+  s->var = var_;
+  s->ints = ints_;
+  s->int_def = int_def_;
+  s->arrs.resize(arrs_.size());
+  for (size_t i = 0; i < arrs_.size(); ++i)
+    if (arrs_[i]) s->arrs[i] = std::make_unique<Arr>(*arrs_[i]);
+  s->iexpr = iexpr_;
+  s->pops = pending_pops_;
+  s->n_slots = n_slots_;
+  s->op_count = op_count;
+  for (int k = 0; k < 8; ++k) s->op_class[k] = op_class_[k];
+  ExecCache& c = exec_cache();
+  std::lock_guard<std::mutex> lk(prog_.exec_mu);
+  if (c.walks.count(key)) return;
+  if (c.walks.size() >= kMaxWalks) {
+    c.walks.erase(c.order.front());
+    c.order.erase(c.order.begin());
+  }
+  c.walks.emplace(key, std::move(s));
+  c.order.push_back(key);
+}
 
 Executor::Executor(Device& dev, const Program& prog, int64_t bitlength, ExecOptions opt)
     : dev_(dev), prog_(prog), opt_(opt) {
@@ -58,7 +157,10 @@ Executor::Executor(Device& dev, const Program& prog, int64_t bitlength, ExecOpti
     fused_ = std::make_unique<FusedBackend>(dev_, opt_);
   flag_buf_ = dev_.alloc_stream(32);
   d_flag_ = reinterpret_cast<unsigned int*>(flag_buf_->p);
-  compute_liveness();
+  ExecCache& c = exec_cache();
+  std::lock_guard<std::mutex> lk(prog_.exec_mu);
+  if (!c.live) c.live = compute_liveness();
+  live_ = c.live;
 }
 
 Executor::~Executor() {
@@ -83,15 +185,25 @@ int64_t Executor::fused_fallbacks() const { return fused_ ? fused_->fallbacks : 
 
 void Executor::set_param(int name, int64_t v) {
   if (name < 0) return;
+  put_raw(bind_sig_, 'p');
+  put_raw(bind_sig_, name);
+  put_raw(bind_sig_, v);
   ints_[name] = IntV{v, -1};
   int_def_[name] = 1;
 }
 
 void Executor::bind_input(int name, BufRef buf, uint8_t tail, bool clean) {
+  put_raw(bind_sig_, 's');
+  put_raw(bind_sig_, name);
+  put_raw(bind_sig_, static_cast<uint8_t>(tail | (clean ? 2 : 0)));
   var_[name] = buf_node(std::move(buf), tail, clean);
 }
 
 void Executor::bind_input_array(int name, int64_t idx, BufRef buf, uint8_t tail, bool clean) {
+  put_raw(bind_sig_, 'a');
+  put_raw(bind_sig_, name);
+  put_raw(bind_sig_, idx);
+  put_raw(bind_sig_, static_cast<uint8_t>(tail | (clean ? 2 : 0)));
   if (!arrs_[name]) arrs_[name] = std::make_unique<Arr>();
   Arr& a = *arrs_[name];
   a.defined = true;
@@ -100,6 +212,10 @@ void Executor::bind_input_array(int name, int64_t idx, BufRef buf, uint8_t tail,
 }
 
 void Executor::bind_broadcast(int name, const std::vector<uint8_t>& ones) {
+  put_raw(bind_sig_, 'b');
+  put_raw(bind_sig_, name);
+  put_raw(bind_sig_, static_cast<int64_t>(ones.size()));
+  bind_sig_.append(reinterpret_cast<const char*>(ones.data()), ones.size());
   if (!arrs_[name]) arrs_[name] = std::make_unique<Arr>();
   Arr& a = *arrs_[name];
   a.defined = true;
@@ -367,8 +483,8 @@ bool Executor::nonzero(int node, const Stmt* at) {
   if (n.op == NOp::Zero) return false;
   if (n.op == NOp::OnesMask || n.op == NOp::AllOnes) return N_ > 0;
   int x = node;
-  auto it = at ? live_at_.find(at->id) : live_at_.end();
-  flush(it == live_at_.end() ? nullptr : &it->second, &x);
+  auto it = at ? live_->at.find(at->id) : live_->at.end();
+  flush(it == live_->at.end() ? nullptr : &it->second, &x);
   BSZ_CUDA(cudaMemsetAsync(d_flag_, 0, 4, dev_.stream()));
   launch_any(dev_, nodes_[x].buf->p, nw_, d_flag_);
   unsigned int h = 0;
@@ -462,8 +578,19 @@ void Executor::run() {
     ran_as_vm_program = true;
     return;
   }
-  exec_block(prog_.stmts);
-  flush(&live_end_, nullptr);
+  // Straight-line programs: restore a cached walk, or walk and cache it when
+  // the walk needed no flush (no popcount forced, no automatic flush).
+  const bool straight = !tracing_ && !has_control_flow(prog_.stmts);
+  std::string key;
+  if (straight) key = walk_key();
+  walk_replayed = straight && replay_walk(key);
+  if (!walk_replayed) {
+    const size_t n0 = nodes_.size();
+    const int64_t f0 = n_flushes_;
+    exec_block(prog_.stmts);
+    if (straight && n_flushes_ == f0) save_walk(key, n0);
+  }
+  flush(&live_->end, nullptr);
   resolve_slots();
   publish_op_mix();
   // Outputs bound to constants get a buffer so the caller can read them.
@@ -494,6 +621,7 @@ void Executor::flush(const Bits* live, int* extra) {
   using clk = std::chrono::steady_clock;
   auto ms_since = [](clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); };
   auto t0 = clk::now();
+  ++n_flushes_;
   const int n_nodes = static_cast<int>(nodes_.size());
   std::vector<uint8_t> is_target(n_nodes, 0), need(n_nodes, 0);
   Segment seg;
@@ -834,7 +962,9 @@ void Executor::resolve_slots() {
 // point).  At a flush only those values are materialized; temporaries that
 // are dead there are never computed.
 
-void Executor::compute_liveness() {
+std::shared_ptr<const Executor::Liveness> Executor::compute_liveness() const {
+  auto live = std::make_shared<Liveness>();
+  auto& live_at = live->at;
   const int nn = static_cast<int>(prog_.names.size());
   const size_t nb = (static_cast<size_t>(nn) + 63) / 64;
   auto scalar = [&](int id) { return id >= 0 && !prog_.is_array[id]; };
@@ -870,7 +1000,7 @@ void Executor::compute_liveness() {
           Bits in = block(s.body, L);
           or_into(L, in);
           set_bit(L, s.e->name);
-          live_at_[s.id] = L;
+          live_at[s.id] = L;
           break;
         }
         case Stmt::While: {
@@ -885,7 +1015,7 @@ void Executor::compute_liveness() {
             if (Xn == X) break;
             X = std::move(Xn);
           }
-          live_at_[s.id] = X;
+          live_at[s.id] = X;
           L = X;
           break;
         }
@@ -908,10 +1038,11 @@ void Executor::compute_liveness() {
     }
     return L;
   };
-  live_end_.assign(nb, 0);
+  live->end.assign(nb, 0);
   for (int id : prog_.outputs)
-    if (scalar(id)) set_bit(live_end_, id);
-  block(prog_.stmts, live_end_);
+    if (scalar(id)) set_bit(live->end, id);
+  block(prog_.stmts, live->end);
+  return live;
 }
 
 // --------------------------------------------------------------- results ---

@@ -111,6 +111,7 @@ class Executor {
   double compile_ms = 0.0;
   int64_t vm_launches = 0;
   bool ran_as_vm_program = false;
+  bool walk_replayed = false;     // the walk came from the program's walk cache
   // Host time split of flushes (ms): building segments, choosing the form,
   // running them (launch + host work; device time overlaps), compacting.
   // Printed to stderr at destruction when $BSZ_HOST_TIMES is set.
@@ -175,9 +176,29 @@ class Executor {
   std::vector<std::pair<int, int64_t>> pending_pops_;
   int64_t resolved_upto_ = 0;
 
-  // liveness: stream names live at each if/while statement
-  std::unordered_map<int, std::vector<uint64_t>> live_at_;
-  std::vector<uint64_t> live_end_;
+  // liveness: stream names live at each if/while statement and at the end
+  // (computed once per program)
+  struct Liveness {
+    std::unordered_map<int, std::vector<uint64_t>> at;
+    std::vector<uint64_t> end;
+  };
+  std::shared_ptr<const Liveness> live_;
+
+  // Walk cache.  A run of a program without if/while whose walk needed no
+  // flush is a deterministic function of the program, the bit length, the
+  // mode and the bindings made before run() (names, tails, cleanliness,
+  // parameters: bind_sig_).  Its result, the DAG and the walk's variable
+  // state, is kept with the program, and a later run with the same key
+  // restores it instead of walking the statements again.  The device work
+  // (every kernel of the flush) runs on every run.
+  struct WalkSnap;
+  struct ExecCache;
+  std::string bind_sig_;
+  int64_t n_flushes_ = 0;
+  ExecCache& exec_cache() const;
+  std::string walk_key() const;
+  bool replay_walk(const std::string& key);
+  void save_walk(const std::string& key, size_t n0);
 
   std::unique_ptr<FusedBackend> fused_;
   unsigned int* d_flag_ = nullptr;
@@ -220,7 +241,7 @@ class Executor {
   const uint64_t* const_ptr(int node);
   void ensure_slots(int64_t need);
   void resolve_slots();
-  void compute_liveness();
+  std::shared_ptr<const Liveness> compute_liveness() const;
   int64_t live_buffer_count() const;
 };
 

@@ -9,6 +9,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
@@ -68,6 +69,10 @@ struct Program {
   std::vector<std::string> names;                          // id -> name
   std::vector<uint8_t> is_array;                           // id -> declared as array
   int n_stmt_ids = 0;
+  // Executor caches of this program (stream liveness, walks of straight-line
+  // runs), created on first use and freed with the program.
+  mutable std::mutex exec_mu;
+  mutable std::shared_ptr<void> exec_cache;
 
   int find(const std::string& s) const {
     auto it = index_.find(s);

@@ -58,6 +58,9 @@ typedef struct bsz_stats {
   int64_t n_fused_launches;  /* generated segment kernels launched */
   int64_t n_fused_fallbacks; /* segment parts re-run per-op because speculation was unproven */
   int64_t n_vm_launches;     /* segments run by the device interpreter */
+  int64_t walk_replayed;     /* 1: a straight-line program's statement walk was restored from
+                                the program's walk cache (same bit length, mode and bindings as
+                                an earlier run); the device work runs in full either way */
 } bsz_stats;
 
 /* Schedule of the generated segment kernels (fused form).  The autotuner and
