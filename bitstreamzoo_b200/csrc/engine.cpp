@@ -108,20 +108,59 @@ bool Executor::replay_walk(const std::string& key) {
   return true;
 }
 
+// The stored walk keeps only the nodes the final flush can reach (from the
+// stream names live at the end, every array element and every pending
+// popcount), renumbered in order; names whose computed value is dead there
+// read -2, as the flush would leave them.  A replay then copies and scans
+// the live DAG only.
 void Executor::save_walk(const std::string& key, size_t n0) {
-  for (size_t i = n0; i < nodes_.size(); ++i)
+  const size_t n = nodes_.size();
+  for (size_t i = n0; i < n; ++i)
     if (nodes_[i].buf) return;   // not a pure walk
+  std::vector<uint8_t> need(n, 0);
+  std::vector<int> stack;
+  auto target = [&](int x) {
+    if (x >= 0) stack.push_back(x);
+  };
+  for (size_t v = 0; v < var_.size(); ++v)
+    if (bit(live_->end, static_cast<int>(v))) target(var_[v]);
+  for (auto& a : arrs_)
+    if (a) for (auto& kv : a->elems) target(kv.second);
+  for (auto& p : pending_pops_) target(p.first);
+  while (!stack.empty()) {
+    int x = stack.back();
+    stack.pop_back();
+    if (need[x]) continue;
+    need[x] = 1;
+    if (nodes_[x].a >= 0) stack.push_back(nodes_[x].a);
+    if (nodes_[x].b >= 0) stack.push_back(nodes_[x].b);
+  }
+  std::vector<int> remap(n, -2);
+  for (size_t i = 0; i < n0; ++i) remap[i] = static_cast<int>(i);
   auto s = std::make_shared<WalkSnap>();
   s->n0 = n0;
-  s->nodes.assign(nodes_.begin() + static_cast<std::ptrdiff_t>(n0), nodes_.end());
-  s->var = var_;
+  for (size_t i = n0; i < n; ++i) {
+    if (!need[i]) continue;
+    remap[i] = static_cast<int>(n0 + s->nodes.size());
+    Node x = nodes_[i];
+    if (x.a >= 0) x.a = remap[x.a];
+    if (x.b >= 0) x.b = remap[x.b];
+    s->nodes.push_back(std::move(x));
+  }
+  auto map = [&](int x) { return x < 0 ? x : remap[x]; };
+  s->var.resize(var_.size());
+  for (size_t v = 0; v < var_.size(); ++v) s->var[v] = map(var_[v]);
   s->ints = ints_;
   s->int_def = int_def_;
   s->arrs.resize(arrs_.size());
   for (size_t i = 0; i < arrs_.size(); ++i)
-    if (arrs_[i]) s->arrs[i] = std::make_unique<Arr>(*arrs_[i]);
+    if (arrs_[i]) {
+      s->arrs[i] = std::make_unique<Arr>(*arrs_[i]);
+      for (auto& kv : s->arrs[i]->elems) kv.second = map(kv.second);
+    }
   s->iexpr = iexpr_;
   s->pops = pending_pops_;
+  for (auto& p : s->pops) p.first = map(p.first);
   s->n_slots = n_slots_;
   s->op_count = op_count;
   for (int k = 0; k < 8; ++k) s->op_class[k] = op_class_[k];
@@ -166,11 +205,13 @@ Executor::Executor(Device& dev, const Program& prog, int64_t bitlength, ExecOpti
 Executor::~Executor() {
   if (std::getenv("BSZ_HOST_TIMES"))
     std::fprintf(stderr,
-                 "[bsz] segments=%lld vm=%lld fused=%lld ops=%lld host ms: segment %.2f policy %.2f run %.2f "
-                 "compact %.2f compile %.2f\n",
+                 "[bsz] segments=%lld vm=%lld fused=%lld ops=%lld replayed=%d host ms: segment %.3f policy %.3f "
+                 "run %.3f (fused prelaunch %.3f wait %.3f) compact %.3f compile %.2f\n",
                  static_cast<long long>(n_segments), static_cast<long long>(vm_launches),
-                 static_cast<long long>(fused_launches()), static_cast<long long>(op_count), t_segment_ms,
-                 t_policy_ms, t_run_ms, t_compact_ms, compile_ms);
+                 static_cast<long long>(fused_launches()), static_cast<long long>(op_count),
+                 walk_replayed ? 1 : 0, t_segment_ms, t_policy_ms, t_run_ms,
+                 fused_ ? fused_->t_prelaunch_ms : 0.0, fused_ ? fused_->t_wait_ms : 0.0, t_compact_ms,
+                 compile_ms);
   cudaStreamSynchronize(dev_.stream());
   // flag, slot and VM buffers go back to the device's cache with their BufRefs
 }

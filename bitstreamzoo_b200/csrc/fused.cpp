@@ -853,8 +853,14 @@ std::unordered_map<std::string, PartKernel>& part_cache() {
   return m;
 }
 
-std::string part_key(const std::vector<Node>& nodes, const Part& p, bool masked, const Schedule& sc) {
+// Key of a node list as the generator reads it: ids, kind, tail,
+// cleanliness, operands, shift amount; then outputs, popcount slots,
+// masking and the schedule.
+std::string graph_key(const std::vector<Node>& nodes, const std::vector<int>& order, const std::vector<int>& inputs,
+                      const std::vector<int>& outputs, const std::vector<std::pair<int, int64_t>>& pops,
+                      bool masked, const Schedule& sc) {
   std::string k;
+  k.reserve(40 * (order.size() + inputs.size()) + 16 * pops.size() + 8 * outputs.size() + 64);
   auto put = [&](int64_t v) { k.append(reinterpret_cast<const char*>(&v), sizeof v); };
   auto node = [&](int n) {
     const Node& x = nodes[n];
@@ -864,14 +870,14 @@ std::string part_key(const std::vector<Node>& nodes, const Part& p, bool masked,
     put(x.b);
     put(x.k);
   };
-  put(static_cast<int64_t>(p.order.size()));
-  for (int n : p.order) node(n);
-  put(static_cast<int64_t>(p.inputs.size()));
-  for (int n : p.inputs) node(n);
-  put(static_cast<int64_t>(p.outputs.size()));
-  for (int n : p.outputs) put(n);
-  put(static_cast<int64_t>(p.pops.size()));
-  for (auto& q : p.pops) {
+  put(static_cast<int64_t>(order.size()));
+  for (int n : order) node(n);
+  put(static_cast<int64_t>(inputs.size()));
+  for (int n : inputs) node(n);
+  put(static_cast<int64_t>(outputs.size()));
+  for (int n : outputs) put(n);
+  put(static_cast<int64_t>(pops.size()));
+  for (auto& q : pops) {
     put(q.first);
     put(q.second);
   }
@@ -879,13 +885,55 @@ std::string part_key(const std::vector<Node>& nodes, const Part& p, bool masked,
   put(sc.warps);
   put(sc.min_blocks);
   put(sc.prefetch);
+  put(sc.cut_adds);
   return k;
+}
+
+std::string part_key(const std::vector<Node>& nodes, const Part& p, bool masked, const Schedule& sc) {
+  return graph_key(nodes, p.order, p.inputs, p.outputs, p.pops, masked, sc);
+}
+
+// A segment's launch plan: its parts (split) with their kernels, keyed by
+// the segment's graph, so a segment seen before is neither split nor keyed
+// part by part again.
+struct SegPlan {
+  std::vector<Part> parts;
+  std::vector<PartKernel> kernels;
+};
+constexpr size_t kMaxPlans = 4096;
+std::mutex g_plan_mu;
+std::unordered_map<std::string, std::shared_ptr<const SegPlan>>& plan_cache() {
+  static std::unordered_map<std::string, std::shared_ptr<const SegPlan>> m;
+  return m;
+}
+
+PartKernel part_kernel(const std::vector<Node>& nodes, const Part& p, int64_t N, const Schedule& sc,
+                       double* compile_ms) {
+  const std::string key = part_key(nodes, p, (N % 64) != 0, sc);
+  {
+    std::lock_guard<std::mutex> lk(g_part_mu);
+    auto it = part_cache().find(key);
+    if (it != part_cache().end()) return it->second;
+  }
+  PartKernel pk;
+  Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
+  const std::string src = g.source();
+  pk.c = compile_source(src, sc.warps * 32, compile_ms);
+  pk.warm = g.warm;
+  std::lock_guard<std::mutex> lk(g_part_mu);
+  part_cache()[key] = pk;
+  return pk;
 }
 
 }  // namespace
 
 bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& seg, int64_t N) {
   const Schedule& sc = impl_->opt.sched;
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    if (plan_cache().count(graph_key(nodes, seg.order, seg.inputs, seg.outputs, seg.pops, (N % 64) != 0, sc)))
+      return true;
+  }
   std::vector<Part> parts = split(nodes, seg, sc.cut_adds != 0);
   for (Part& p : parts) {
     if (p.order.empty() && p.pops.empty()) continue;
@@ -906,29 +954,32 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
   Device& dev = impl_->dev;
   const ExecOptions& opt = impl_->opt;
   const Schedule& sc = opt.sched;
-  std::vector<Part> parts = split(nodes, seg, sc.cut_adds != 0);
-  for (Part& p : parts) {
-    if (p.order.empty() && p.pops.empty()) continue;
-    if (p.inputs.size() > kMaxInputs) throw RuntimeError("fused: too many inputs in one segment");
-    const std::string key = part_key(nodes, p, (N % 64) != 0, sc);
-    PartKernel pk;
-    bool hit = false;
-    {
-      std::lock_guard<std::mutex> lk(g_part_mu);
-      auto it = part_cache().find(key);
-      if (it != part_cache().end()) {
-        pk = it->second;
-        hit = true;
-      }
+  using clk = std::chrono::steady_clock;
+  auto ms_since = [](clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); };
+  auto tp = clk::now();
+  const std::string skey = graph_key(nodes, seg.order, seg.inputs, seg.outputs, seg.pops, (N % 64) != 0, sc);
+  std::shared_ptr<const SegPlan> plan;
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    auto it = plan_cache().find(skey);
+    if (it != plan_cache().end()) plan = it->second;
+  }
+  if (!plan) {
+    auto np = std::make_shared<SegPlan>();
+    for (Part& p : split(nodes, seg, sc.cut_adds != 0)) {
+      if (p.order.empty() && p.pops.empty()) continue;
+      if (p.inputs.size() > kMaxInputs) throw RuntimeError("fused: too many inputs in one segment");
+      np->kernels.push_back(part_kernel(nodes, p, N, sc, compile_ms));
+      np->parts.push_back(std::move(p));
     }
-    if (!hit) {
-      Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
-      const std::string src = g.source();
-      pk.c = compile_source(src, sc.warps * 32, compile_ms);
-      pk.warm = g.warm;
-      std::lock_guard<std::mutex> lk(g_part_mu);
-      part_cache()[key] = pk;
-    }
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    if (plan_cache().size() >= kMaxPlans) plan_cache().clear();
+    plan_cache()[skey] = np;
+    plan = np;
+  }
+  for (size_t pi = 0; pi < plan->parts.size(); ++pi) {
+    const Part& p = plan->parts[pi];
+    const PartKernel& pk = plan->kernels[pi];
     const Compiled& c = pk.c;
     // outputs
     for (int n : p.outputs)
@@ -966,9 +1017,13 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
     }
     ++dev.n_launches;
     ++launches;
+    t_prelaunch_ms += ms_since(tp);
+    auto tw = clk::now();
     unsigned int fail = 0;
     BSZ_CUDA(cudaMemcpyAsync(&fail, impl_->d_fail, 4, cudaMemcpyDeviceToHost, dev.stream()));
     BSZ_CUDA(cudaStreamSynchronize(dev.stream()));
+    t_wait_ms += ms_since(tw);
+    tp = clk::now();
     if (fail) {
       // Speculation could not be proven exact: redo this part with the plain
       // per-op kernels (exact by construction).

@@ -29,6 +29,9 @@ class FusedBackend {
 
   int64_t fallbacks = 0;   // parts re-run with the plain kernels (speculation unproven)
   int64_t launches = 0;    // fused kernels launched
+  // Host time (ms) in run(): before each launch returns (split, kernel
+  // lookup or generation, arguments, launch) and waiting for the kernel.
+  double t_prelaunch_ms = 0, t_wait_ms = 0;
 
   struct Impl;
 
