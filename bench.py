@@ -58,9 +58,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-op comparison form")
-    ap.add_argument("--schedule", default="model", choices=["model", "model1", "default"],
-                    help="fused-kernel schedule: the fastest of the shipped cost model's 4 best predictions "
-                         "(timed during warm-up), its top-1 pick (no timing), or the default")
+    ap.add_argument("--schedule", default="tuned", choices=["tuned", "model", "model1", "default"],
+                    help="fused-kernel schedule: the autotuner's pick (every candidate of the 16-schedule "
+                         "space timed before the timed region), the fastest of the shipped cost model's 4 "
+                         "best predictions, the model's top-1 pick (no timing), or the default")
     return ap.parse_args()
 
 
@@ -334,7 +335,13 @@ def run_ours(args, rank, world, local):
         return reduce_max(x, dist, dev)
 
     sched, sched_src = dict(bz.DEFAULT_SCHEDULE), "default"
-    if args.schedule in ("model", "model1"):
+    if args.schedule == "tuned":
+        from bitstreamzoo_b200 import tuner
+        ins = {k: (t.data_ptr(), nw) for k, t in dev_in.items()}
+        sched = tuner.Autotuner(ctx).best(prog, W.src, nbits, ins)
+        sched_src = (f"autotuner: fastest of all {len(tuner.CANDIDATES)} candidates "
+                     "(median of 3 device-timed runs each, before the timed region)")
+    elif args.schedule in ("model", "model1"):
         from bitstreamzoo_b200 import tuner
         model = tuner.CostModel.load_default(ctx)
         if model is not None and args.schedule == "model1":

@@ -57,7 +57,7 @@ enum class ExecMode : int { Plain = 0, Fused = 1, Auto = 2, Vm = 3 };
 struct Schedule {
   int warps = 4;          // warps per CTA
   int range_steps = 64;   // minimum 32-word steps per warp range (words per tile / 32)
-  int ctas_per_sm = 0;    // resident CTAs per SM; 0 = as many as the kernel's occupancy allows
+  int ctas_per_sm = 0;    // resident CTAs per SM; 0 = as many as the kernel's occupancy allows; -1 = no cap (one minimum-length range per warp)
   int min_blocks = 4;     // __launch_bounds__ minimum blocks (caps registers per thread)
   int prefetch = 1;       // issue the next step's loads before the current step's arithmetic
   int cut_adds = 0;       // 1: every addition ends a part (its result is materialized)

@@ -37,6 +37,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <set>
@@ -132,7 +133,7 @@ void FusedBackend::set_schedule(const Schedule& s) {
   Schedule c = s;
   c.warps = std::max(1, std::min(c.warps, 16));
   c.range_steps = std::max(1, c.range_steps);
-  c.ctas_per_sm = std::max(0, c.ctas_per_sm);
+  c.ctas_per_sm = std::max(-1, c.ctas_per_sm);
   c.min_blocks = std::max(1, std::min(c.min_blocks, 32));
   impl_->opt.sched = c;
 }
@@ -997,7 +998,10 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
     const int64_t steps = (nw + 31) / 32;
     // persistent grid: as many warps as the compiled kernel keeps resident
     const int per_sm = sc.ctas_per_sm > 0 ? std::min(sc.ctas_per_sm, c.blocks_per_sm) : c.blocks_per_sm;
-    int64_t max_warps = static_cast<int64_t>(dev.sm_count()) * per_sm * sc.warps;
+    // ctas_per_sm < 0: no persistent cap, every warp takes one range of the
+    // minimum length (more warps, shorter ranges, more warm-up work)
+    const int64_t max_warps = sc.ctas_per_sm < 0 ? std::numeric_limits<int64_t>::max() / 2
+                                                 : static_cast<int64_t>(dev.sm_count()) * per_sm * sc.warps;
     int64_t min_range_steps = std::max<int64_t>(sc.range_steps, (pk.warm / 32) * 8);
     int64_t warps_needed = std::max<int64_t>(1, std::min(max_warps, (steps + min_range_steps - 1) / min_range_steps));
     int64_t range = ((steps + warps_needed - 1) / warps_needed) * 32;

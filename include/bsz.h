@@ -69,7 +69,8 @@ typedef struct bsz_stats {
 typedef struct bsz_schedule {
   int32_t warps;        /* warps per CTA (1..16) */
   int32_t range_steps;  /* minimum 32-word steps owned by one warp (words per tile / 32) */
-  int32_t ctas_per_sm;  /* resident CTAs per SM, 0 = as many as occupancy allows */
+  int32_t ctas_per_sm;  /* resident CTAs per SM, 0 = as many as occupancy allows, -1 = no
+                           persistent cap: one minimum-length range per warp */
   int32_t min_blocks;   /* launch-bounds minimum blocks per SM (caps registers) */
   int32_t prefetch;     /* 1: load the next 32-word step before computing this one */
   int32_t cut_adds;     /* 1: materialize every addition (one kernel per addition level) */

@@ -113,7 +113,11 @@ def test_every_candidate_schedule_is_bit_exact(ctx):
     r.execute()
     want = {f"o{j}": r.stream(f"o{j}") for j in range(4)}
     want_i = {f"p{j}": r.int(f"p{j}") for j in range(4)}
-    for s in tuner.CANDIDATES:
+    # the candidate space, plus the uncapped grid (ctas_per_sm = -1: one
+    # minimum-length range per warp) at two range lengths
+    extra = [dict(bz.DEFAULT_SCHEDULE, ctas_per_sm=-1, range_steps=rs, prefetch=pf)
+             for rs in (1, 64) for pf in (0, 1)]
+    for s in list(tuner.CANDIDATES) + extra:
         f = prog.run(nbits, bz.MODE_FUSED)
         f.set_schedule(s)
         for k, v in ins.items():
