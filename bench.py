@@ -219,6 +219,18 @@ class Clocks:
 
 # ---------------------------------------------------------------- CPU side --
 
+def cpu_model() -> str:
+    """The host CPU's model name (as lscpu reports it), or "unknown"."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(workload: str, nbits: int, reps: int, warm: int = 1):
     """Reference CPU executor (bsim --backend simd_omp, AVX-512 + OpenMP, all
     host threads) on a bounded sample of the workload; falls back to the C
@@ -259,6 +271,7 @@ def cpu_baseline(workload: str, nbits: int, reps: int, warm: int = 1):
             # the reference's single-core AVX-512 form, once, beside it
             ms1 = run_bsim("simd", 1, 0)
         return {"value": w.in_bytes / (ms * 1e-3) / 1e9, "unit": "GB/s", "cores": threads,
+                "cpu_model": cpu_model(),
                 "single_core": {"value": w.in_bytes / (ms1 * 1e-3) / 1e9, "unit": "GB/s", "cores": 1,
                                 "backend": "bsim --backend simd", "ms": ms1},
                 "kind": "reference", "ms_per_step": ms,
@@ -275,7 +288,7 @@ def cpu_baseline(workload: str, nbits: int, reps: int, warm: int = 1):
             times.append((time.perf_counter() - t0) * 1e3)
     ms = statistics.median(times)
     return {"value": w.in_bytes / (ms * 1e-3) / 1e9, "unit": "GB/s",
-            "cores": cwords.lib().o_num_threads(), "kind": "port", "ms_per_step": ms,
+            "cores": cwords.lib().o_num_threads(), "cpu_model": cpu_model(), "kind": "port", "ms_per_step": ms,
             "sample": f"{workload} at {nbits} bits per stream, oracle C port, median of {len(times)}"}
 
 
@@ -452,7 +465,7 @@ def run_ours(args, rank, world, local):
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cb = cpu_baseline(args.workload, args.cpu_sample_bits or DEFAULT_CPU_SAMPLE[args.workload], 3)
+            cb = cpu_baseline(args.workload, args.cpu_sample_bits or DEFAULT_CPU_SAMPLE[args.workload], 5)
         except Exception as e:  # noqa: BLE001
             cb = {"unavailable": str(e)[:200]}
 
