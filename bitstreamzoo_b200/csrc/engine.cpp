@@ -401,7 +401,7 @@ int Executor::read_var(int name) {
   int n = var_[name];
   if (n >= 0) return n;
   if (n == -2)
-    throw RuntimeError("internal: variable '" + prog_.names[name] + "' read after being judged dead");
+    throw RuntimeError("internal: variable '" + prog_.names[name] + "' read after being found dead");
   throw RuntimeError("undefined stream variable: " + prog_.names[name]);
 }
 

@@ -22,7 +22,7 @@ stream length, so it is searched, not fixed:
   or measures only the ``top_k`` best predictions.
 
 The model is fitted on a random sample of the (program, length, schedule)
-timings of training programs and judged on held-out programs by pick regret:
+timings of training programs and evaluated on held-out programs by pick regret:
 time of the picked schedule / time of the exhaustive best - 1.
 """
 
