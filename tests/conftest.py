@@ -60,7 +60,18 @@ def mask_outputs(out, ints, nbits):
     return res
 
 
-REFERENCE_TREE = os.environ.get("BSZ_REFERENCE_TREE", "/root/reference")
+def _reference_tree():
+    # the oracle recipe holds the one definition of the reference tree location
+    v = os.environ.get("BSZ_REFERENCE_TREE")
+    if v:
+        return v
+    import subprocess
+    oracle_dir = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle")
+    r = subprocess.run(["make", "-s", "-C", oracle_dir, "print-ref"], capture_output=True, text=True)
+    return r.stdout.strip() if r.returncode == 0 else ""
+
+
+REFERENCE_TREE = _reference_tree()
 has_reference = os.path.isdir(os.path.join(REFERENCE_TREE, "simulator", "pythonsim"))
 
 

@@ -1,8 +1,10 @@
 """Generate the committed golden vectors from the reference implementation.
 
-Run in a container that has the reference tree (default /root/reference):
+Run in a container that has the reference tree (its location: --ref, else
+$BSZ_REFERENCE_TREE, else the oracle recipe's default, ``make -s -C oracle
+print-ref``):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <reference tree>]
 
 Every expected value is produced by the reference's normative Python
 interpreter (simulator/pythonsim/interpreter.py), imported from the reference
@@ -250,11 +252,20 @@ def gen_tail_corners(ref: Ref):
     return recs
 
 
+def reference_tree():
+    v = os.environ.get("BSZ_REFERENCE_TREE")
+    if v:
+        return v
+    oracle_dir = os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle")
+    return subprocess.run(["make", "-s", "-C", oracle_dir, "print-ref"], capture_output=True, text=True,
+                          check=True).stdout.strip()
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None)
     args = ap.parse_args()
-    ref = Ref(args.ref)
+    ref = Ref(args.ref or reference_tree())
     groups = {"random_programs": gen_random(ref), "kat_ops": gen_kats(ref),
               "tail_corners": gen_tail_corners(ref)}
     try:
