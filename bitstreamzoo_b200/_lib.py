@@ -106,6 +106,7 @@ SIGNATURES = {
     "bsz_op_popcount": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_uint64, u64p]),
     "bsz_add_noalloc": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_uint64, ctypes.c_int64,
                                        c_void_p]),
+    "bsz_debug_add_lookback_hook": (None, [ctypes.c_int64, ctypes.c_int]),
     "bsz_s2p": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, ctypes.POINTER(c_void_p)]),
     "bsz_op_is_nonzero": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_uint64,
                                          ctypes.POINTER(ctypes.c_int)]),

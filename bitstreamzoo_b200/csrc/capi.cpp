@@ -153,7 +153,7 @@ int bsz_sync(bsz_ctx* ctx) {
   return guard([&] {
     ctx->dev->sync();
     if (uint32_t e = ctx->dev->take_error())
-      throw bsz::RuntimeError("device error word " + std::to_string(e));
+      throw bsz::RuntimeError(bsz::describe_device_error(e));
   });
 }
 
@@ -573,7 +573,7 @@ int bsz_batch_finish(bsz_batch* b, bsz_stats* stats) {
   return guard([&] {
     b->runner->finish();
     if (uint32_t e = b->ctx->dev->take_error())
-      throw bsz::RuntimeError("device error word " + std::to_string(e));
+      throw bsz::RuntimeError(bsz::describe_device_error(e));
     if (stats) {
       std::memset(stats, 0, sizeof(*stats));
       stats->n_kernel_launches = b->ctx->dev->n_launches - b->launches0;
@@ -637,8 +637,19 @@ const char* bsz_run_case_json(bsz_ctx* ctx, const char* source, const char* bsda
 }
 
 // ---- per-op data plane --------------------------------------------------
+namespace {
+// The logical length of an op on n words: 0 means the full storage width
+// (64 n bits, the C++ binaries' convention); otherwise 1 .. 64 n.
+uint64_t checked_mask(const char* op, int64_t bitlength, uint64_t n) {
+  if (bitlength < 0 || (bitlength > 0 && static_cast<uint64_t>(bitlength) > 64 * n))
+    throw std::invalid_argument(std::string(op) + ": bitlength " + std::to_string(bitlength) +
+                                " outside [0, 64 * n_words] for n_words = " + std::to_string(n));
+  return bsz::mask_for_bits(bitlength);
+}
+}  // namespace
+
 int bsz_op_not(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, uint64_t n, int64_t bitlength) {
-  return guard([&] { bsz::launch_not(*ctx->dev, dst, a, n, bsz::mask_for_bits(bitlength)); });
+  return guard([&] { bsz::launch_not(*ctx->dev, dst, a, n, checked_mask("bsz_op_not", bitlength, n)); });
 }
 int bsz_op_and(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b, uint64_t n) {
   return guard([&] { bsz::launch_bitwise(*ctx->dev, bsz::kAnd, dst, a, b, n); });
@@ -654,13 +665,15 @@ int bsz_op_andnot(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t
 }
 int bsz_op_add(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b, uint64_t n,
                int64_t bitlength) {
-  return guard([&] { bsz::launch_add(*ctx->dev, dst, a, b, n, bsz::mask_for_bits(bitlength)); });
+  return guard([&] {
+    bsz::launch_add(*ctx->dev, dst, a, b, n, checked_mask("bsz_op_add", bitlength, n));
+  });
 }
 int bsz_op_shl(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, uint64_t k, uint64_t n,
                int64_t bitlength) {
   return guard([&] {
     bsz::launch_shl(*ctx->dev, dst, a, static_cast<int64_t>(std::min<uint64_t>(k, uint64_t(1) << 62)), n,
-                    bsz::mask_for_bits(bitlength));
+                    checked_mask("bsz_op_shl", bitlength, n));
   });
 }
 int bsz_op_shr(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, uint64_t k, uint64_t n, int tail) {
@@ -685,6 +698,10 @@ int bsz_s2p(bsz_ctx* ctx, const uint8_t* bytes, int64_t n_bytes, uint64_t* const
     if (n_bytes > 0 && (!bytes || !basis)) throw bsz::RuntimeError("bsz_s2p: null pointer");
     bsz::launch_s2p(*ctx->dev, bytes, n_bytes, basis);
   });
+}
+
+void bsz_debug_add_lookback_hook(int64_t silent_tile, int spin_limit) {
+  bsz::set_add_lookback_test_hook(silent_tile, spin_limit);
 }
 
 int bsz_op_is_nonzero(bsz_ctx* ctx, const uint64_t* a, uint64_t n, int* result) {

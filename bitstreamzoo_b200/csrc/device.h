@@ -32,6 +32,16 @@ enum : uint32_t {
   kErrFusedOverflow = 1u << 2,     // fused kernel: halo/state capacity exceeded
 };
 
+// Human-readable text of a nonzero device error word.
+inline std::string describe_device_error(uint32_t e) {
+  std::string s = "device error word " + std::to_string(e) + ":";
+  if (e & kErrLookbackTimeout) s += " carry look-back timed out;";
+  if (e & kErrFusedTimeout) s += " fused-kernel wait timed out;";
+  if (e & kErrFusedOverflow) s += " fused-kernel state capacity exceeded;";
+  s.pop_back();
+  return s;
+}
+
 class Device;
 
 // A device stream buffer of n_words uint64 words (256-byte aligned).  Freed
@@ -161,6 +171,10 @@ int64_t add_state_words(int64_t n);
 // look-back state (add_state_words(n) zeroed words) and error word.
 void launch_add_on_stream(cudaStream_t stream, uint64_t* d, const uint64_t* a, const uint64_t* b,
                           int64_t n, uint64_t last_mask, uint32_t* state, uint32_t* err);
+// Test hook of the add kernel's look-back: tile `silent_tile` never publishes
+// its status and every wait gives up after `spin_limit` spins (<= 0: the
+// default limit).  silent_tile = -1 turns the hook off.
+void set_add_lookback_test_hook(int64_t silent_tile, int spin_limit);
 void launch_popcount(Device& dev, const uint64_t* a, int64_t n,
                      unsigned long long* slot);
 void launch_any(Device& dev, const uint64_t* a, int64_t n, unsigned int* flag);

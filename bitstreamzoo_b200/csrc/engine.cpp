@@ -532,7 +532,7 @@ bool Executor::nonzero(int node, const Stmt* at) {
   BSZ_CUDA(cudaMemcpyAsync(&h, d_flag_, 4, cudaMemcpyDeviceToHost, dev_.stream()));
   dev_.sync();
   ++n_syncs;
-  if (uint32_t err = dev_.take_error()) throw RuntimeError("device error word " + std::to_string(err));
+  if (uint32_t err = dev_.take_error()) throw RuntimeError(describe_device_error(err));
   return h != 0;
 }
 
@@ -649,7 +649,7 @@ void Executor::run() {
     if (arrs_[id])
       for (auto& kv : arrs_[id]->elems) materialize(kv.second);
   }
-  if (uint32_t err = dev_.take_error()) throw RuntimeError("device error word " + std::to_string(err));
+  if (uint32_t err = dev_.take_error()) throw RuntimeError(describe_device_error(err));
 }
 
 // ----------------------------------------------------------------- flush ---

@@ -8,7 +8,8 @@
 //   AND/OR/XOR/ANDNOT/NOT   16 B vector loads, 4 in flight per thread
 //   SHL/SHR                 one output word per lane, the neighbour word
 //                           comes from L1 (both loads are warp-coalesced)
-//   ADD                     single pass: per-warp ballot carry resolution
+//   ADD                     single pass: 4-word blocks per lane (256-bit
+//                           accesses), per-warp ballot carry resolution
 //                           + decoupled look-back across CTAs (24 B/word,
 //                           the reference's CUB scan path moves ~120 B/word)
 //   POPCOUNT / ANY          one pass, one atomic per CTA, no host sync
@@ -177,24 +178,35 @@ k_shr(uint64_t* __restrict__ d, const uint64_t* __restrict__ a, int64_t ws, int 
 }
 
 // ---- add: single-pass carry scan ----------------------------------------
-// A CTA of kAddWarps warps owns one tile of kAddTile consecutive words; each
-// warp owns kAddSteps consecutive 32-word steps of it (lane = word in step,
-// so every load/store is a coalesced 256-byte warp access).
+// A CTA of kAddWarps warps owns one tile of kAddTile consecutive words.  Each
+// warp owns kAddSteps consecutive 128-word steps of it; in a step, lane l
+// owns the 4-word block at 4l: one 32-byte sector, a 256-bit load or store
+// per lane, so every warp access is one contiguous kilobyte.
 //
-// Carry resolution inside a step: with per-lane generate g (the word sum
-// overflowed) and propagate p (the word sum is all ones), the carries into
-// the 32 lanes are the internal carries of the 32-bit addition
-// (G|P) + G + cin; carry into lane i = bit i of ((G|P)+G+cin) ^ P, carry out =
-// bit 32.  Across steps and warps the (g, p) pairs compose; across CTAs the
-// tile aggregate is published and resolved by decoupled look-back (status
-// word = flag | g | p<<1), with bounded spins.
+// Carry resolution inside a step: per block, generate g (the block sum with
+// no carry in overflowed) and propagate p (a ^ b is all ones over the block:
+// then, and only then, the carry out equals the carry in).  The carries into
+// the 32 blocks are the internal carries of the 32-bit addition
+// (G|P) + G + cin: carry into lane i = bit i of ((G|P)+G+cin) ^ P, carry out
+// = bit 32.  Across steps and warps the (g, p) pairs compose; across CTAs the
+// tile aggregate is published as soon as the tile's loads have landed and is
+// resolved by decoupled look-back (status word = flag | g | p<<1), with
+// bounded spins.  dst may be a or b exactly (each word is read before it is
+// written, by the one thread that writes it); partial overlaps are not
+// allowed.
 constexpr int kAddWarps = 8;
-constexpr int kAddSteps = 8;
-constexpr int64_t kAddTile = kAddWarps * kAddSteps * 32;
+constexpr int kAddSteps = 4;
+constexpr int64_t kAddTile = kAddWarps * kAddSteps * 128;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kFlagMask = 3u << 30;
 constexpr int kSpinLimit = 1 << 22;
+
+// Test hook: a tile that never publishes its status, and a shorter spin
+// limit, so a test can make a look-back wait run out (its successor then
+// reports kErrLookbackTimeout).  Off (-1, kSpinLimit) unless a test sets it.
+int64_t g_add_silent_tile = -1;
+int g_add_spin_limit = kSpinLimit;
 
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
   return *reinterpret_cast<const volatile uint32_t*>(p);
@@ -203,9 +215,83 @@ __device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) {
   *reinterpret_cast<volatile uint32_t*>(p) = v;
 }
 
+// 4 words at word index w (w % 4 == 0): one 256-bit load when the block is
+// whole and the pointer 32-byte aligned, else word by word (zero past n).
+// Plain (coherent) loads: dst may alias the operand.
+template <bool VEC>
+__device__ __forceinline__ void load4(const uint64_t* p, int64_t w, int64_t n, uint64_t r[4]) {
+  if (VEC && w + 3 < n) {
+    asm volatile("ld.global.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(r[0]), "=l"(r[1]), "=l"(r[2]), "=l"(r[3])
+                 : "l"(p + w));
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) r[i] = (w + i < n) ? p[w + i] : 0;
+  }
+}
+
+template <bool VEC>
+__device__ __forceinline__ void store4(uint64_t* p, int64_t w, int64_t n, const uint64_t r[4]) {
+  if (VEC && w + 3 < n) {
+    asm volatile("st.global.v4.u64 [%0], {%1,%2,%3,%4};" ::"l"(p + w), "l"(r[0]), "l"(r[1]), "l"(r[2]),
+                 "l"(r[3])
+                 : "memory");
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (w + i < n) p[w + i] = r[i];
+  }
+}
+
+#define BSZ_LO(x) static_cast<uint32_t>(x)
+#define BSZ_HI(x) static_cast<uint32_t>((x) >> 32)
+
+// s = a + b over a 256-bit block (no carry in); returns the carry out.
+__device__ __forceinline__ uint32_t add4(uint64_t s[4], const uint64_t a[4], const uint64_t b[4]) {
+  uint32_t r[8], c;
+  asm("add.cc.u32 %0, %9, %17;\n\t"
+      "addc.cc.u32 %1, %10, %18;\n\t"
+      "addc.cc.u32 %2, %11, %19;\n\t"
+      "addc.cc.u32 %3, %12, %20;\n\t"
+      "addc.cc.u32 %4, %13, %21;\n\t"
+      "addc.cc.u32 %5, %14, %22;\n\t"
+      "addc.cc.u32 %6, %15, %23;\n\t"
+      "addc.cc.u32 %7, %16, %24;\n\t"
+      "addc.u32 %8, 0, 0;"
+      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5]), "=&r"(r[6]),
+        "=&r"(r[7]), "=&r"(c)
+      : "r"(BSZ_LO(a[0])), "r"(BSZ_HI(a[0])), "r"(BSZ_LO(a[1])), "r"(BSZ_HI(a[1])), "r"(BSZ_LO(a[2])),
+        "r"(BSZ_HI(a[2])), "r"(BSZ_LO(a[3])), "r"(BSZ_HI(a[3])), "r"(BSZ_LO(b[0])), "r"(BSZ_HI(b[0])),
+        "r"(BSZ_LO(b[1])), "r"(BSZ_HI(b[1])), "r"(BSZ_LO(b[2])), "r"(BSZ_HI(b[2])), "r"(BSZ_LO(b[3])),
+        "r"(BSZ_HI(b[3])));
+#pragma unroll
+  for (int i = 0; i < 4; ++i) s[i] = (static_cast<uint64_t>(r[2 * i + 1]) << 32) | r[2 * i];
+  return c;
+}
+
+// s += c (c in {0, 1}) over a 256-bit block.
+__device__ __forceinline__ void inc4(uint64_t s[4], uint32_t c) {
+  uint32_t r[8];
+  asm("add.cc.u32 %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, 0;\n\t"
+      "addc.cc.u32 %2, %10, 0;\n\t"
+      "addc.cc.u32 %3, %11, 0;\n\t"
+      "addc.cc.u32 %4, %12, 0;\n\t"
+      "addc.cc.u32 %5, %13, 0;\n\t"
+      "addc.cc.u32 %6, %14, 0;\n\t"
+      "addc.u32 %7, %15, 0;"
+      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5]), "=&r"(r[6]),
+        "=&r"(r[7])
+      : "r"(BSZ_LO(s[0])), "r"(BSZ_HI(s[0])), "r"(BSZ_LO(s[1])), "r"(BSZ_HI(s[1])), "r"(BSZ_LO(s[2])),
+        "r"(BSZ_HI(s[2])), "r"(BSZ_LO(s[3])), "r"(BSZ_HI(s[3])), "r"(c));
+#pragma unroll
+  for (int i = 0; i < 4; ++i) s[i] = (static_cast<uint64_t>(r[2 * i + 1]) << 32) | r[2 * i];
+}
+
+template <bool VEC>
 __global__ void __launch_bounds__(kAddWarps * 32)
-k_add(uint64_t* __restrict__ d, const uint64_t* __restrict__ a, const uint64_t* __restrict__ b,
-      int64_t n, uint64_t last_mask, uint32_t* __restrict__ state, uint32_t* __restrict__ err) {
+k_add(uint64_t* d, const uint64_t* a, const uint64_t* b, int64_t n, uint64_t last_mask,
+      uint32_t* __restrict__ state, uint32_t* __restrict__ err, int64_t silent_tile, int spin_limit) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_wagg[kAddWarps];
   __shared__ uint32_t s_cin;
@@ -213,26 +299,32 @@ k_add(uint64_t* __restrict__ d, const uint64_t* __restrict__ a, const uint64_t* 
   __syncthreads();
   const int64_t tile = s_tile;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t wbase = tile * kAddTile + static_cast<int64_t>(warp) * kAddSteps * 32 + lane;
-  uint64_t sum[kAddSteps];
+  const int64_t wbase = tile * kAddTile + static_cast<int64_t>(warp) * (kAddSteps * 128) + 4 * lane;
+  uint64_t sum[kAddSteps][4];
   uint32_t G[kAddSteps], P[kAddSteps];
+  {
+    uint64_t x[kAddSteps][4], y[kAddSteps][4];
 #pragma unroll
-  for (int j = 0; j < kAddSteps; ++j) {
-    int64_t w = wbase + j * 32;
-    uint64_t x = 0, y = 0;
-    if (w < n) { x = a[w]; y = b[w]; }
-    uint64_t s = x + y;
-    sum[j] = s;
-    G[j] = __ballot_sync(0xffffffffu, s < x);
-    P[j] = __ballot_sync(0xffffffffu, w < n && s == ~uint64_t(0));
+    for (int j = 0; j < kAddSteps; ++j) {
+      load4<VEC>(a, wbase + j * 128, n, x[j]);
+      load4<VEC>(b, wbase + j * 128, n, y[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < kAddSteps; ++j) {
+      const uint32_t g = add4(sum[j], x[j], y[j]);
+      const uint64_t q = (x[j][0] ^ y[j][0]) & (x[j][1] ^ y[j][1]) & (x[j][2] ^ y[j][2]) & (x[j][3] ^ y[j][3]);
+      G[j] = __ballot_sync(0xffffffffu, g != 0);
+      // words past n are zero in both operands, so their blocks never propagate
+      P[j] = __ballot_sync(0xffffffffu, q == ~uint64_t(0));
+    }
   }
   // warp aggregate over its steps (in word order)
   uint32_t wg = 0, wp = 1;
 #pragma unroll
   for (int j = 0; j < kAddSteps; ++j) {
-    uint64_t z = static_cast<uint64_t>(G[j] | P[j]) + G[j];
-    uint32_t sg = static_cast<uint32_t>(z >> 32);
-    uint32_t sp = P[j] == 0xffffffffu;
+    const uint64_t z = static_cast<uint64_t>(G[j] | P[j]) + G[j];
+    const uint32_t sg = static_cast<uint32_t>(z >> 32);
+    const uint32_t sp = P[j] == 0xffffffffu;
     wg = sg | (sp & wg);
     wp &= sp;
   }
@@ -242,34 +334,44 @@ k_add(uint64_t* __restrict__ d, const uint64_t* __restrict__ a, const uint64_t* 
     uint32_t tg = 0, tp = 1;
 #pragma unroll
     for (int w = 0; w < kAddWarps; ++w) {
-      uint32_t g = s_wagg[w] & 1u, p = s_wagg[w] >> 1;
+      const uint32_t g = s_wagg[w] & 1u, p = s_wagg[w] >> 1;
       tg = g | (p & tg);
       tp &= p;
     }
     uint32_t* status = state + 1;
     uint32_t cin = 0;
-    if (tile == 0) {
-      if (lane == 0) st_volatile(&status[0], kFlagInc | tg);
-    } else {
-      if (lane == 0) {
+    if (lane == 0 && tile != silent_tile) {
+      if (tile == 0) {
+        st_volatile(&status[0], kFlagInc | tg);
+      } else {
         st_volatile(&status[tile], kFlagAgg | tg | (tp << 1));
-        // walk back: acc = composition of the tiles between j and this one
+        // walk back: (ag, ap) = composition of the tiles between j and this one
         uint32_t ag = 0, ap = 1;
         int64_t j = tile - 1;
         int spins = 0;
         while (true) {
-          uint32_t v = ld_volatile(&status[j]);
-          uint32_t f = v & kFlagMask;
+          const uint32_t v = ld_volatile(&status[j]);
+          const uint32_t f = v & kFlagMask;
           if (f == 0) {
-            if (++spins > kSpinLimit) { atomicOr(err, kErrLookbackTimeout); cin = 0; break; }
+            if (++spins > spin_limit) {
+              atomicOr(err, kErrLookbackTimeout);
+              cin = 0;
+              break;
+            }
             __nanosleep(32);
             continue;
           }
-          if (f == kFlagInc) { cin = ag | (ap & (v & 1u)); break; }
-          uint32_t g = v & 1u, p = (v >> 1) & 1u;
+          if (f == kFlagInc) {
+            cin = ag | (ap & (v & 1u));
+            break;
+          }
+          const uint32_t g = v & 1u, p = (v >> 1) & 1u;
           ag = ag | (ap & g);
           ap &= p;
-          if (!ap) { cin = ag; break; }   // carry out of the range no longer depends on earlier tiles
+          if (!ap) {   // the carry out of the walked range no longer depends on earlier tiles
+            cin = ag;
+            break;
+          }
           --j;
           spins = 0;
         }
@@ -282,22 +384,29 @@ k_add(uint64_t* __restrict__ d, const uint64_t* __restrict__ a, const uint64_t* 
   __syncthreads();
   uint32_t c = s_cin;
   for (int w = 0; w < warp; ++w) {
-    uint32_t g = s_wagg[w] & 1u, p = s_wagg[w] >> 1;
+    const uint32_t g = s_wagg[w] & 1u, p = s_wagg[w] >> 1;
     c = g | (p & c);
   }
 #pragma unroll
   for (int j = 0; j < kAddSteps; ++j) {
-    uint64_t z = static_cast<uint64_t>(G[j] | P[j]) + G[j] + c;
-    uint32_t carries = static_cast<uint32_t>(z) ^ P[j];
+    const uint64_t z = static_cast<uint64_t>(G[j] | P[j]) + G[j] + c;
+    const uint32_t carries = static_cast<uint32_t>(z) ^ P[j];
     c = static_cast<uint32_t>(z >> 32);
-    int64_t w = wbase + j * 32;
+    const int64_t w = wbase + j * 128;
     if (w < n) {
-      uint64_t r = sum[j] + ((carries >> lane) & 1u);
-      if (w == n - 1) r &= last_mask;
-      d[w] = r;
+      inc4(sum[j], (carries >> lane) & 1u);
+      if (w + 3 >= n - 1) {   // this block holds the last word
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (w + i == n - 1) sum[j][i] &= last_mask;
+      }
+      store4<VEC>(d, w, n, sum[j]);
     }
   }
 }
+
+#undef BSZ_LO
+#undef BSZ_HI
 
 // ---- reductions ------------------------------------------------------------
 __device__ __forceinline__ uint64_t warp_sum(uint64_t v) {
@@ -400,24 +509,36 @@ void launch_shr(Device& dev, uint64_t* d, const uint64_t* a, int64_t k, int64_t 
 
 int64_t add_state_words(int64_t n) { return 1 + (n + kAddTile - 1) / kAddTile; }
 
+static bool aligned32(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 31) == 0; }
+
+static void launch_add_kernel(cudaStream_t stream, uint64_t* d, const uint64_t* a, const uint64_t* b,
+                              int64_t n, uint64_t last_mask, uint32_t* state, uint32_t* err) {
+  const int64_t tiles = (n + kAddTile - 1) / kAddTile;
+  if (tiles > 0x7fffffff) throw std::invalid_argument("launch_add: stream too long");
+  const bool vec = aligned32(d) && aligned32(a) && aligned32(b);
+  auto k = vec ? k_add<true> : k_add<false>;
+  k<<<static_cast<unsigned>(tiles), kAddWarps * 32, 0, stream>>>(d, a, b, n, last_mask, state, err,
+                                                                  g_add_silent_tile, g_add_spin_limit);
+  check_launch();
+}
+
 void launch_add_with_state(Device& dev, uint64_t* d, const uint64_t* a, const uint64_t* b,
                            int64_t n, uint64_t last_mask, uint32_t* state) {
   if (n <= 0) return;
-  int64_t tiles = (n + kAddTile - 1) / kAddTile;
-  if (tiles > 0x7fffffff) throw std::invalid_argument("launch_add: stream too long");
   ProfScope prof(dev, "k_add");
-  k_add<<<static_cast<unsigned>(tiles), kAddWarps * 32, 0, dev.stream()>>>(
-      d, a, b, n, last_mask, state, dev.error_word());
-  check_launch();
+  launch_add_kernel(dev.stream(), d, a, b, n, last_mask, state, dev.error_word());
   ++dev.n_launches;
 }
 
 void launch_add_on_stream(cudaStream_t stream, uint64_t* d, const uint64_t* a, const uint64_t* b,
                           int64_t n, uint64_t last_mask, uint32_t* state, uint32_t* err) {
   if (n <= 0) return;
-  int64_t tiles = (n + kAddTile - 1) / kAddTile;
-  k_add<<<static_cast<unsigned>(tiles), kAddWarps * 32, 0, stream>>>(d, a, b, n, last_mask, state, err);
-  check_launch();
+  launch_add_kernel(stream, d, a, b, n, last_mask, state, err);
+}
+
+void set_add_lookback_test_hook(int64_t silent_tile, int spin_limit) {
+  g_add_silent_tile = silent_tile;
+  g_add_spin_limit = spin_limit > 0 ? spin_limit : kSpinLimit;
 }
 
 void launch_add(Device& dev, uint64_t* d, const uint64_t* a, const uint64_t* b, int64_t n,

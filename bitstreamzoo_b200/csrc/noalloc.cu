@@ -10,7 +10,14 @@
 // bsz_op_add(), but its look-back scratch (one status word per 2048-word
 // tile, a tile ticket and an error word) lives in a fixed-size file-scope
 // __device__ array instead of memory from cudaMalloc.  Every GPU that loads
-// the library holds this array (about 129 KiB) until the process exits.
+// the library's device code holds this array (about 129 KiB) until the
+// process exits.  The CUDA runtime loads that code on a device lazily, at the
+// first kernel launch or symbol lookup there, and that load commits the
+// array: it is the one device allocation this entry point causes, and it
+// happens on its first call on each device.  A caller that must not allocate
+// later makes that first call at start-up (a call with n_words = 0 does only
+// the set-up), while allocation is still allowed and before any stream
+// capture.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -67,11 +74,19 @@ uint32_t* scratch_on_current_device() {
 extern "C" int bsz_add_noalloc(uint64_t* dst, const uint64_t* a, const uint64_t* b, uint64_t n_words,
                                int64_t bitlength, void* stream) {
   try {
-    if (n_words == 0) return 0;
+    if (n_words == 0) {
+      // set-up only: load this library's device code on the current device
+      // (which commits the scratch array) and look up the array's address
+      scratch_on_current_device();
+      return 0;
+    }
     if (n_words > static_cast<uint64_t>(kMaxWords))
       throw std::invalid_argument("bsz_add_noalloc: n_words = " + std::to_string(n_words) +
                                   " exceeds the maximum of " + std::to_string(kMaxWords) +
                                   " words (2^32 bits); use bsz_op_add for longer streams");
+    if (bitlength < 0 || (bitlength > 0 && static_cast<uint64_t>(bitlength) > 64 * n_words))
+      throw std::invalid_argument("bsz_add_noalloc: bitlength " + std::to_string(bitlength) +
+                                  " outside [0, 64 * n_words] for n_words = " + std::to_string(n_words));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     uint32_t* scratch = scratch_on_current_device();
     const int64_t n = static_cast<int64_t>(n_words);

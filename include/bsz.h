@@ -198,9 +198,11 @@ const char* bsz_run_case_json(bsz_ctx* ctx, const char* source, const char* bsda
 
 /* ---- per-op data plane on device pointers (CudaBackend op_*) -----------
  * dst/a/b are device pointers to n_words words; `bitlength` is the logical
- * length (bits at and above it are cleared by ~, + and <<).  All calls are
- * asynchronous on the context's stream except popcount / is_nonzero, which
- * return their result to the host. */
+ * length (bits at and above it are cleared by ~, + and <<): 1 .. 64*n_words,
+ * or 0 for the full storage width; anything else is an error.  dst may be
+ * a or b exactly (in place); partially overlapping buffers are not allowed.
+ * All calls are asynchronous on the context's stream except popcount /
+ * is_nonzero, which return their result to the host. */
 int bsz_op_not(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, uint64_t n_words,
                int64_t bitlength);
 int bsz_op_and(bsz_ctx* ctx, uint64_t* dst, const uint64_t* a, const uint64_t* b,
@@ -234,17 +236,30 @@ int bsz_s2p(bsz_ctx* ctx, const uint8_t* bytes, int64_t n_bytes, uint64_t* const
  * application that passes its own buffers through FFI and owns every
  * allocation, or a loop that cannot pay for the device-wide synchronisation
  * of cudaMalloc/cudaFree.  Same result as bsz_op_add (dst = a + b with bits
- * at and above `bitlength` cleared); no context is needed.  The look-back
- * scratch is a fixed file-scope device array of about 129 KiB that every GPU
- * loading the library keeps until exit, so n_words is limited to 2^26
- * (streams of up to 2^32 bits); longer streams are rejected with an error.
- * The first call on a device looks up that array's address (do it before
- * any stream capture).  Every call reuses the same array, so calls that
- * overlap on the GPU (different streams, or different host threads) race;
- * serialize them.  Runs on `stream` (a cudaStream_t, NULL for the default
- * stream) and returns when the addition has finished. */
+ * at and above `bitlength` cleared; the same bitlength and in-place rules);
+ * no context is needed.  The look-back scratch is a fixed file-scope device
+ * array of about 129 KiB, so n_words is limited to 2^26 (streams of up to
+ * 2^32 bits); longer streams are rejected with an error.  The CUDA runtime
+ * loads the library's device code on a device lazily, and that load commits
+ * the array, which the device then keeps until the process exits: the first
+ * call on each device therefore allocates those 129 KiB once.  Callers that
+ * must never allocate later make one set-up call per device at start-up,
+ * while allocation is still allowed and before any stream capture; a call
+ * with n_words = 0 does only that set-up (pointers unused).  Every call
+ * reuses the same array, so calls that overlap on the GPU (different
+ * streams, or different host threads) race; serialize them.  Runs on
+ * `stream` (a cudaStream_t, NULL for the default stream) and returns when
+ * the addition has finished. */
 int bsz_add_noalloc(uint64_t* dst, const uint64_t* a, const uint64_t* b, uint64_t n_words,
                     int64_t bitlength, void* stream);
+
+/* Test hook for the add kernel's bounded look-back waits (no counterpart in
+ * the reference; tests only).  Until reset with silent_tile = -1, tile
+ * `silent_tile` of every add never publishes its carry status and a wait
+ * gives up after `spin_limit` spins (<= 0: the normal limit), so the tile
+ * after it reports a look-back timeout: bsz_op_add's context and
+ * bsz_add_noalloc then return an error naming it.  Not thread-safe. */
+void bsz_debug_add_lookback_hook(int64_t silent_tile, int spin_limit);
 
 #ifdef __cplusplus
 }

@@ -147,3 +147,71 @@ def test_unaligned_pointers_take_scalar_path(ctx):
     ctx.sync()
     assert np.array_equal(host(dd)[1:], (a ^ b)[1:])
     assert ctx.popcount(da.data_ptr() + off, n) == cwords.popcount(a[1:])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["a", "b"])
+def test_add_in_place(ctx, which):
+    """dst may be one of the operands: every word is read before it is written."""
+    n = 3 * 4096 + 5
+    rng = np.random.default_rng(17)
+    a, b = rand_words(rng, n), rand_words(rng, n)
+    a[100:2000] = np.uint64(2**64 - 1)   # a propagate run across a block boundary
+    b[99] = np.uint64(2**64 - 1)
+    da, db = dev(a), dev(b)
+    torch.cuda.synchronize()
+    dst = da if which == "a" else db
+    ctx.op("add", dst.data_ptr(), da.data_ptr(), db.data_ptr(), n, 64 * n - 3)
+    ctx.sync()
+    assert np.array_equal(host(dst), cwords.add(a, b, 64 * n - 3))
+
+
+@pytest.mark.gpu
+def test_add_unaligned_multi_tile(ctx):
+    """8-byte-aligned (not 32-byte-aligned) operands take the word-by-word path."""
+    n = 2 * 4096 + 77
+    rng = np.random.default_rng(23)
+    a, b = rand_words(rng, n + 1), rand_words(rng, n + 1)
+    a[1:3000] = np.uint64(2**64 - 1)
+    b[1] = np.uint64(1)
+    da, db = dev(a), dev(b)
+    dd = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    off = 8
+    ctx.op("add", dd.data_ptr() + off, da.data_ptr() + off, db.data_ptr() + off, n, 64 * n)
+    ctx.sync()
+    assert np.array_equal(host(dd)[1:], cwords.add(a[1:], b[1:], 64 * n))
+
+
+@pytest.mark.gpu
+def test_add_rejects_bitlength_outside_the_words(ctx):
+    from bitstreamzoo_b200 import _lib
+    n = 64
+    d = torch.zeros(n, dtype=torch.int64, device="cuda")
+    for bad in (-1, 64 * n + 1):
+        with pytest.raises(_lib.BszError, match="bitlength"):
+            ctx.op("add", d.data_ptr(), d.data_ptr(), d.data_ptr(), n, bad)
+
+
+@pytest.mark.gpu
+def test_add_lookback_timeout_is_reported(ctx):
+    """A look-back wait that runs out (its predecessor tile never publishes,
+    through the test hook) ends with an error the host reads; the context
+    stays usable and the next add is exact."""
+    from bitstreamzoo_b200 import _lib
+    lib = _lib.load()
+    n = 4 * 4096
+    rng = np.random.default_rng(29)
+    a, b = rand_words(rng, n), rand_words(rng, n)
+    da, db, dd = dev(a), dev(b), torch.empty(n, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    lib.bsz_debug_add_lookback_hook(1, 1000)
+    try:
+        ctx.op("add", dd.data_ptr(), da.data_ptr(), db.data_ptr(), n, 64 * n)
+        with pytest.raises(_lib.BszError, match="look-back timed out"):
+            ctx.sync()
+    finally:
+        lib.bsz_debug_add_lookback_hook(-1, 0)
+    ctx.op("add", dd.data_ptr(), da.data_ptr(), db.data_ptr(), n, 64 * n)
+    ctx.sync()
+    assert np.array_equal(host(dd), cwords.add(a, b, 64 * n))

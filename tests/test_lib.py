@@ -132,3 +132,12 @@ def test_cli_dump_input_large_stream_hex(tmp_path):
     d = json.loads(out.stdout)
     assert d["inputs"]["a"] == hex(a)
     assert int(d["inputs"]["b"], 16) == b
+
+
+def test_noalloc_add_rejects_bitlength_outside_its_words():
+    # checked before any device call, so this runs without a GPU
+    lib = _lib.load()
+    dummy = ctypes.c_void_p(16)
+    for bad in (-5, 64 * 10 + 1):
+        assert lib.bsz_add_noalloc(dummy, dummy, dummy, 10, bad, None) != 0
+        assert "bitlength" in _lib.last_error()
