@@ -32,7 +32,7 @@ MODE_VM = 3
 MODES = {"plain": MODE_PLAIN, "fused": MODE_FUSED, "auto": MODE_AUTO, "vm": MODE_VM}
 
 DEFAULT_SCHEDULE = {"warps": 4, "range_steps": 64, "ctas_per_sm": 0, "min_blocks": 4,
-                    "prefetch": 1, "cut_adds": 0}
+                    "prefetch": 1, "cut_adds": 0, "layout": 0}
 
 __all__ = ["Context", "Program", "Run", "B200Backend", "BszError", "MODE_PLAIN", "MODE_FUSED",
            "MODE_AUTO", "MODE_VM",
@@ -102,10 +102,13 @@ class Context:
         return Program(self, source)
 
     def run(self, source, bitlength: int, inputs=None, params=None, input_arrays=None,
-            broadcast=None, mode: int = MODE_PLAIN):
-        """Compile + run; returns a finished ``Run``."""
+            broadcast=None, mode: int = MODE_PLAIN, schedule: dict | None = None):
+        """Compile + run; returns a finished ``Run``.  ``schedule``: fused
+        kernel knobs over DEFAULT_SCHEDULE (see ``Run.set_schedule``)."""
         prog = source if isinstance(source, Program) else self.compile(source)
         r = prog.run(bitlength, mode)
+        if schedule:
+            r.set_schedule(schedule)
         for k, v in (params or {}).items():
             r.set_param(k, v)
         for k, v in (inputs or {}).items():

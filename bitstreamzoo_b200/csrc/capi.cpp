@@ -217,6 +217,7 @@ int bsz_run_set_schedule(bsz_run* run, const bsz_schedule* s) {
     c.min_blocks = s->min_blocks;
     c.prefetch = s->prefetch;
     c.cut_adds = s->cut_adds;
+    c.layout = s->layout;
     executor(run).set_schedule(c);
   });
 }

@@ -61,6 +61,7 @@ struct Schedule {
   int min_blocks = 4;     // __launch_bounds__ minimum blocks (caps registers per thread)
   int prefetch = 1;       // issue the next step's loads before the current step's arithmetic
   int cut_adds = 0;       // 1: every addition ends a part (its result is materialized)
+  int layout = 0;         // 0: warp ranges, lane = word; 1: thread-sequential ranges
 };
 
 struct ExecOptions {

@@ -135,6 +135,7 @@ void FusedBackend::set_schedule(const Schedule& s) {
   c.range_steps = std::max(1, c.range_steps);
   c.ctas_per_sm = std::max(-1, c.ctas_per_sm);
   c.min_blocks = std::max(1, std::min(c.min_blocks, 32));
+  c.layout = c.layout ? 1 : 0;
   impl_->opt.sched = c;
 }
 
@@ -642,6 +643,395 @@ struct Gen {
   }
 };
 
+// Thread-sequential form of a segment part.  Each thread owns a contiguous
+// range of whole 4-word chunks and walks it in word order, so every
+// cross-word operator keeps its state in the thread's registers:
+//   * x + y: a 64-bit add with carry in and out (a PTX carry chain: four
+//     integer instructions per word), the carry held in a register;
+//   * x << k (k < 64): two funnel shifts against the previous word of x,
+//     held in a register (a temporary shifted by 64 bits or more ends the
+//     part: it is materialized by an earlier kernel);
+//   * shifts of an input by 64 bits or more read the input at the word
+//     offset directly.
+// Memory: a chunk of every input is one 256-bit load per thread (one 32-byte
+// sector), a chunk of every output one 256-bit store; the chunks of
+// neighbouring threads are a range apart.  Chunks at the ends of the stream
+// (and any chunk whose shifted loads would leave [0, nw)) take a scalar path
+// with bounds, tail fill and last-word masking.  The state at the start of a
+// thread's range comes from speculation as in the warp form: H warm-up words
+// from an all-zero state, per-node dirt tracking (an addition is exact after
+// the first word where a ^ b is not all ones, at or after its operands' dirt),
+// doubled up to 8 times, then the fail flag and the exact per-op fallback.
+struct GenSeq {
+  const std::vector<Node>& nodes;
+  const Part& part;
+  int64_t N;
+  int warps;
+  int min_blocks;
+  bool masked;
+  std::map<int, int> in_idx;
+  std::vector<std::pair<int, int>> outs;
+  std::set<int> in_part;
+  std::set<int> prev_src;            // nodes whose previous word a shift (k < 64) reads
+  std::vector<uint8_t> dyn;
+  std::map<int, int64_t> sdh;        // static dirt (words) of nodes without add ancestors
+  int64_t warm = 4;                  // warm-up words (multiple of 4)
+  std::vector<int> emit_order;
+  // shifted input reads by a word offset: (node, word offset) -> slot; the
+  // offset is -ws for a left shift and +ws for a right shift (|ws| >= 1 for
+  // left shifts; right shifts also read offset ws + 1)
+  std::map<std::pair<int, int64_t>, int> off_slot;
+  int64_t fast_lo = 0;               // a chunk at c is fast if c >= fast_lo ...
+  int64_t fast_hi_pad = 3;           // ... and c + fast_hi_pad <= nw - 1 - masked
+
+  std::string v(int n) const { return "v" + std::to_string(n); }
+
+  void analyze() {
+    for (size_t i = 0; i < part.inputs.size(); ++i) in_idx[part.inputs[i]] = static_cast<int>(i);
+    for (size_t i = 0; i < part.outputs.size(); ++i) outs.push_back({part.outputs[i], static_cast<int>(i)});
+    for (int n : part.order) in_part.insert(n);
+    dyn.assign(nodes.size(), 0);
+    int64_t max_static = 0;
+    for (int n : part.order) {
+      const Node& x = nodes[n];
+      auto d = [&](int o) -> int64_t { return (o >= 0 && sdh.count(o)) ? sdh[o] : 0; };
+      bool dy = x.op == NOp::Add;
+      for (int o : {x.a, x.b})
+        if (o >= 0 && dyn[o]) dy = true;
+      int64_t s = std::max(d(x.a), d(x.b));
+      if (x.op == NOp::Shl) {
+        const int64_t ws = x.k / 64;
+        if (in_part.count(x.a)) {
+          if (ws > 0) throw RuntimeError("fused: shift of a temporary by 64 bits or more in a sequential part");
+          if (x.k > 0) { prev_src.insert(x.a); s = d(x.a) + 1; }
+        } else if (!is_const(nodes[x.a].op)) {
+          if (ws == 0) {
+            // the previous word of an input is exact from the second warm-up word on
+            if (x.k > 0) { prev_src.insert(x.a); s = 1; }
+          } else {
+            off_slot[{x.a, -ws}] = 0;
+            if (x.k % 64) off_slot[{x.a, -ws - 1}] = 0;
+          }
+        }
+      } else if (x.op == NOp::Shr && !is_const(nodes[x.a].op)) {
+        const int64_t ws = x.k / 64;
+        off_slot[{x.a, ws}] = 0;
+        if (x.k % 64) off_slot[{x.a, ws + 1}] = 0;
+      }
+      dyn[n] = dy;
+      if (!dy) {
+        sdh[n] = s;
+        max_static = std::max(max_static, s);
+      }
+    }
+    warm = std::max<int64_t>(4, ((max_static + 2 + 3) / 4) * 4);
+    int k = 0;
+    for (auto& kv : off_slot) {
+      kv.second = k++;
+      // a fast chunk at c loads words [c + base, c + base + 8) for this slot
+      const int64_t off = kv.first.second, base = slot_base(off);
+      if (base < 0) fast_lo = std::max<int64_t>(fast_lo, -base);
+      else fast_hi_pad = std::max<int64_t>(fast_hi_pad, base + 7);
+    }
+    order_for_registers();
+  }
+
+  void order_for_registers() {
+    std::map<int, int> users;
+    std::map<int, int64_t> size;
+    for (int n : part.order) {
+      const Node& x = nodes[n];
+      int64_t sz = 1;
+      for (int o : {x.a, x.b})
+        if (o >= 0 && in_part.count(o)) {
+          ++users[o];
+          sz += size[o];
+        }
+      size[n] = std::min<int64_t>(sz, int64_t(1) << 40);
+    }
+    std::set<int> seen;
+    auto visit = [&](int root) {
+      std::vector<std::pair<int, int>> st{{root, 0}};
+      while (!st.empty()) {
+        auto& [n, stage] = st.back();
+        if (stage == 0) {
+          if (seen.count(n)) { st.pop_back(); continue; }
+          seen.insert(n);
+          stage = 1;
+          const Node& x = nodes[n];
+          std::vector<int> kids;
+          for (int o : {x.a, x.b})
+            if (o >= 0 && in_part.count(o) && !seen.count(o)) kids.push_back(o);
+          if (kids.size() == 2 && size[kids[0]] < size[kids[1]]) std::swap(kids[0], kids[1]);
+          for (auto it = kids.rbegin(); it != kids.rend(); ++it) st.push_back({*it, 0});
+        } else {
+          emit_order.push_back(n);
+          st.pop_back();
+        }
+      }
+    };
+    std::vector<int> roots;
+    for (auto& o : outs) roots.push_back(o.first);
+    for (auto& p : part.pops) roots.push_back(p.first);
+    for (int n : part.order)
+      if (!users.count(n)) roots.push_back(n);
+    for (int r : roots)
+      if (in_part.count(r)) visit(r);
+    for (int n : part.order)
+      if (!seen.count(n)) visit(n);
+  }
+
+  // Bounded scalar read of word `idx` of an input or constant node.
+  std::string ld(int n, const std::string& idx) const {
+    const Node& x = nodes[n];
+    if (x.op == NOp::Zero) return "0ull";
+    if (x.op == NOp::AllOnes) return "((" + idx + ") >= 0 ? ~0ull : 0ull)";
+    if (x.op == NOp::OnesMask)
+      return "((" + idx + ") >= 0 && (" + idx + ") < A.nw - 1 ? ~0ull : ((" + idx +
+             ") == A.nw - 1 ? A.last_mask : 0ull))";
+    const std::string fill = x.tail ? "~0ull" : "0ull";
+    return "((" + idx + ") >= 0 && (" + idx + ") < A.nw ? A.in[" + std::to_string(in_idx.at(n)) + "][" + idx +
+           "] : " + fill + ")";
+  }
+
+  // Value of an input/constant at the current word in the fast path.
+  std::string fast_in(int n, int j) const {
+    const Node& x = nodes[n];
+    if (x.op == NOp::Zero) return "0ull";
+    if (x.op == NOp::AllOnes || x.op == NOp::OnesMask) return "~0ull";   // the fast path never holds the last word
+    return "c" + std::to_string(in_idx.at(n)) + "_" + std::to_string(j);
+  }
+  // Word at offset `off` of input n (a shifted read), fast path: from the two
+  // aligned chunks loaded for that slot.
+  // first word (relative to the chunk) of the two aligned chunks loaded for
+  // word offset `off`: they hold words j + off for j = 0..3
+  static int64_t slot_base(int64_t off) { return off < 0 ? -4 * ((-off + 3) / 4) : 4 * (off / 4); }
+  std::string fast_off(int n, int64_t off, int j) const {
+    const int slot = off_slot.at({n, off});
+    return "o" + std::to_string(slot) + "_" + std::to_string(j + off - slot_base(off));
+  }
+
+  // One word of the DAG.  mode 'f': fast (word j of the chunk at c);
+  // 's': scalar at word w; 't': scalar with dirt tracking (warm-up, relative
+  // word r).  Values only; the caller stores / counts.
+  void emit_word(std::ostringstream& s, char mode, int j) const {
+    const bool slow = mode != 'f';
+    const std::string W = slow ? "w" : "(c + " + std::to_string(j) + ")";
+    if (slow && masked) s << "      const u64 lm = (w == A.nw - 1) ? A.last_mask : ~0ull;\n";
+    for (auto& kv : in_idx) {
+      if (is_const(nodes[kv.first].op) && !slow) continue;
+      s << "      const u64 " << v(kv.first) << " = " << (slow ? ld(kv.first, "w") : fast_in(kv.first, j)) << ";\n";
+    }
+    auto opnd = [&](int o) -> std::string {
+      if (!slow && is_const(nodes[o].op)) return fast_in(o, j);
+      return v(o);
+    };
+    auto word_at = [&](int n, int64_t off) -> std::string {
+      if (slow) return ld(n, "w + (" + std::to_string(off) + "ll)");
+      return fast_off(n, off, j);
+    };
+    for (int n : emit_order) {
+      const Node& x = nodes[n];
+      const std::string a = x.a >= 0 ? opnd(x.a) : "", b = x.b >= 0 ? opnd(x.b) : "";
+      const bool mask_here = slow && masked;
+      switch (x.op) {
+        case NOp::Not: s << "      const u64 " << v(n) << " = ~" << a << (mask_here ? " & lm" : "") << ";\n"; break;
+        case NOp::And: s << "      const u64 " << v(n) << " = " << a << " & " << b << ";\n"; break;
+        case NOp::Or: s << "      const u64 " << v(n) << " = " << a << " | " << b << ";\n"; break;
+        case NOp::Xor: s << "      const u64 " << v(n) << " = " << a << " ^ " << b << ";\n"; break;
+        case NOp::AndNot:
+          s << "      const u64 " << v(n) << " = " << a << " & ~" << b << (mask_here ? " & lm" : "") << ";\n";
+          break;
+        case NOp::Add:
+          if (mode == 't' && dyn[n])
+            s << "      if (!res" << n << " && r >= max(" << dh(x.a) << ", " << dh(x.b) << ") && (" << a << " ^ " << b
+              << ") != ~0ull) { res" << n << " = 1; dh" << n << " = r + 1; }\n";
+          s << "      const u64 " << v(n) << " = addc(" << a << ", " << b << ", cy" << n << ")"
+            << (mask_here ? " & lm" : "") << ";\n";
+          break;
+        case NOp::Shl: {
+          const int64_t ws = x.k / 64;
+          const int bs = static_cast<int>(x.k % 64);
+          std::string e;
+          if (x.k == 0) e = a;
+          else if (ws == 0 && !is_const(nodes[x.a].op)) e = "fshl<" + std::to_string(bs) + ">(" + a + ", pv" + std::to_string(x.a) + ")";
+          else if (is_const(nodes[x.a].op)) {
+            // a constant shifted left: word w is the constant's word w - ws (and w - ws - 1)
+            const std::string lo = ld(x.a, W + " - " + std::to_string(ws) + "ll");
+            e = bs ? "fshl<" + std::to_string(bs) + ">(" + lo + ", " + ld(x.a, W + " - " + std::to_string(ws + 1) + "ll") + ")" : lo;
+          } else {
+            const std::string lo = word_at(x.a, -ws);
+            e = bs ? "fshl<" + std::to_string(bs) + ">(" + lo + ", " + word_at(x.a, -ws - 1) + ")" : lo;
+          }
+          s << "      const u64 " << v(n) << " = " << e << (mask_here ? " & lm" : "") << ";\n";
+          break;
+        }
+        case NOp::Shr: {
+          const int64_t ws = x.k / 64;
+          const int bs = static_cast<int>(x.k % 64);
+          std::string e;
+          if (is_const(nodes[x.a].op)) {
+            const std::string lo = ld(x.a, W + " + " + std::to_string(ws) + "ll");
+            e = bs ? "fshr<" + std::to_string(bs) + ">(" + lo + ", " + ld(x.a, W + " + " + std::to_string(ws + 1) + "ll") + ")" : lo;
+          } else {
+            const std::string lo = word_at(x.a, ws);
+            e = bs ? "fshr<" + std::to_string(bs) + ">(" + lo + ", " + word_at(x.a, ws + 1) + ")" : lo;
+          }
+          s << "      const u64 " << v(n) << " = " << e << ";\n";
+          break;
+        }
+        default:
+          throw RuntimeError("fused: unexpected node kind");
+      }
+      if (mode == 't' && dyn[n] && x.op != NOp::Add) {
+        if (x.op == NOp::Shl && in_part.count(x.a) && x.k > 0)
+          s << "      dh" << n << " = min(" << dh(x.a) << " + 1, 1 << 30);\n";
+        else
+          s << "      dh" << n << " = max(" << dh(x.a) << ", " << dh(x.b) << ");\n";
+      }
+    }
+    // previous words for the next word's shifts (after every use in this word)
+    for (int n : prev_src) s << "      pv" << n << " = " << (in_part.count(n) ? v(n) : opnd(n)) << ";\n";
+  }
+
+  std::string dh(int o) const {
+    if (o < 0 || !in_part.count(o)) return "0";
+    if (dyn[o]) return "dh" + std::to_string(o);
+    auto it = sdh.find(o);
+    return std::to_string(it == sdh.end() ? 0 : it->second);
+  }
+
+  void emit_store_word(std::ostringstream& s) const {
+    for (auto& kv : outs) s << "      A.out[" << kv.second << "][w] = " << v(kv.first) << ";\n";
+    for (size_t j = 0; j < part.pops.size(); ++j) s << "      pc" << j << " += __popcll(" << v(part.pops[j].first) << ");\n";
+  }
+
+  std::string source() {
+    analyze();
+    std::ostringstream s;
+    const int ni = static_cast<int>(part.inputs.size()), no = static_cast<int>(part.outputs.size());
+    s << Gen::args_struct(ni, no);
+    s << "template <int K> __device__ __forceinline__ u64 fshl(u64 x, u64 p) {\n"
+         "  const u32 xl = (u32)x, xh = (u32)(x >> 32), pl = (u32)p, ph = (u32)(p >> 32);\n"
+         "  u32 lo, hi;\n"
+         "  if constexpr (K < 32) { lo = __funnelshift_l(ph, xl, K); hi = __funnelshift_l(xl, xh, K); }\n"
+         "  else if constexpr (K == 32) { lo = ph; hi = xl; }\n"
+         "  else { lo = __funnelshift_l(pl, ph, K - 32); hi = __funnelshift_l(ph, xl, K - 32); }\n"
+         "  return ((u64)hi << 32) | lo;\n}\n"
+         "template <int K> __device__ __forceinline__ u64 fshr(u64 x, u64 nx) {\n"
+         "  const u32 xl = (u32)x, xh = (u32)(x >> 32), nl = (u32)nx, nh = (u32)(nx >> 32);\n"
+         "  u32 lo, hi;\n"
+         "  if constexpr (K < 32) { lo = __funnelshift_r(xl, xh, K); hi = __funnelshift_r(xh, nl, K); }\n"
+         "  else if constexpr (K == 32) { lo = xh; hi = nl; }\n"
+         "  else { lo = __funnelshift_r(xh, nl, K - 32); hi = __funnelshift_r(nl, nh, K - 32); }\n"
+         "  return ((u64)hi << 32) | lo;\n}\n"
+         "__device__ __forceinline__ u64 addc(u64 a, u64 b, u32& c) {\n"
+         "  u32 lo, hi, co;\n"
+         "  asm(\"{ .reg .u32 t;\\n\\tadd.cc.u32 t, %3, 0xffffffff;\\n\\taddc.cc.u32 %0, %4, %6;\\n\\t\"\n"
+         "      \"addc.cc.u32 %1, %5, %7;\\n\\taddc.u32 %2, 0, 0;\\n\\t}\"\n"
+         "      : \"=&r\"(lo), \"=&r\"(hi), \"=r\"(co)\n"
+         "      : \"r\"(c), \"r\"((u32)a), \"r\"((u32)(a >> 32)), \"r\"((u32)b), \"r\"((u32)(b >> 32)));\n"
+         "  c = co;\n  return ((u64)hi << 32) | lo;\n}\n"
+         "__device__ __forceinline__ void ld4(const u64* p, u64& a, u64& b, u64& c, u64& d) {\n"
+         "  asm volatile(\"ld.global.nc.L2::128B.v4.u64 {%0,%1,%2,%3}, [%4];\" : \"=l\"(a), \"=l\"(b), \"=l\"(c), \"=l\"(d) : \"l\"(p));\n}\n"
+         "__device__ __forceinline__ void st4(u64* p, u64 a, u64 b, u64 c, u64 d) {\n"
+         "  asm volatile(\"st.global.v4.u64 [%0], {%1,%2,%3,%4};\" :: \"l\"(p), \"l\"(a), \"l\"(b), \"l\"(c), \"l\"(d) : \"memory\");\n}\n";
+    s << "extern \"C\" __global__ void __launch_bounds__(" << warps * 32 << ", " << min_blocks
+      << ")\nbsz_fused(const Args A) {\n"
+      << "  const int lane = threadIdx.x & 31;\n"
+      << "  const long long s = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * A.range;\n"
+      << "  const bool active = s < A.nw;\n"
+      << "  const long long e = min(s + A.range, A.nw);\n";
+    std::vector<int> adds;
+    for (int n : part.order)
+      if (nodes[n].op == NOp::Add) adds.push_back(n);
+    for (int n : adds) s << "  u32 cy" << n << " = 0;\n";
+    for (int n : prev_src) s << "  u64 pv" << n << " = 0;\n";
+    for (size_t j = 0; j < part.pops.size(); ++j) s << "  u32 pc" << j << " = 0;\n";
+    s << "  if (active) {\n";
+    // ---- warm-up
+    if (!adds.empty() || !prev_src.empty()) {
+      s << "  long long p0 = s - " << warm << "ll;\n  if (p0 < 0) p0 = 0;\n"
+        << "  for (int attempt = 0; p0 < s; ++attempt) {\n";
+      for (int n : adds) s << "    cy" << n << " = 0;\n";
+      for (int n : prev_src) s << "    pv" << n << " = 0;\n";
+      for (int n : adds)
+        if (dyn[n]) s << "    int res" << n << " = (p0 == 0);\n    int dh" << n << " = (p0 == 0) ? 0 : (1 << 30);\n";
+      for (int n : part.order)
+        if (dyn[n] && nodes[n].op != NOp::Add) s << "    int dh" << n << " = 0;\n";
+      s << "    for (long long w = p0; w < s; ++w) {\n      const int r = (int)(w - p0);\n";
+      emit_word(s, 't', 0);
+      s << "    }\n    const int need = (int)(s - p0);\n    bool ok = true;\n";
+      for (int n : adds)
+        if (dyn[n]) s << "    ok = ok && res" << n << " && dh" << n << " <= need;\n";
+      for (int n : prev_src) {
+        if (!in_part.count(n)) continue;
+        if (dyn[n]) s << "    ok = ok && dh" << n << " <= need - 1;\n";
+        else if (sdh.count(n) && sdh.at(n) > 0) s << "    ok = ok && " << sdh.at(n) << " <= need - 1;\n";
+      }
+      s << "    if (ok || p0 == 0) break;\n"
+        << "    if (attempt >= 8) { atomicOr(A.fail, 1u); break; }\n"
+        << "    p0 = s - 2 * (s - p0);\n    if (p0 < 0) p0 = 0;\n"
+        << "  }\n";
+    }
+    // ---- owned range
+    const int pad = static_cast<int>(fast_hi_pad) + (masked && fast_hi_pad == 3 ? 1 : 0);
+    s << "  long long w = s;\n"
+      << "  const long long fast_end = A.nw - 1 - " << pad << "ll;   // a fast chunk at c needs c <= fast_end\n"
+      << "  while (w < e) {\n"
+      << "    if (w + 4 <= e && w >= " << fast_lo << "ll && w <= fast_end) {\n"
+      << "      const long long c = w;\n";
+    for (auto& kv : in_idx) {
+      if (is_const(nodes[kv.first].op)) continue;
+      const std::string i = std::to_string(kv.second);
+      s << "      u64 c" << i << "_0, c" << i << "_1, c" << i << "_2, c" << i << "_3;\n"
+        << "      ld4(A.in[" << i << "] + c, c" << i << "_0, c" << i << "_1, c" << i << "_2, c" << i << "_3);\n";
+    }
+    for (auto& kv : off_slot) {
+      const int n = kv.first.first;
+      const int64_t base = slot_base(kv.first.second);
+      const std::string sl = std::to_string(kv.second), i = std::to_string(in_idx.at(n));
+      s << "      u64 o" << sl << "_0, o" << sl << "_1, o" << sl << "_2, o" << sl << "_3, o" << sl << "_4, o" << sl
+        << "_5, o" << sl << "_6, o" << sl << "_7;\n"
+        << "      ld4(A.in[" << i << "] + c + (" << base << "ll), o" << sl << "_0, o" << sl << "_1, o" << sl << "_2, o"
+        << sl << "_3);\n"
+        << "      ld4(A.in[" << i << "] + c + (" << base + 4 << "ll), o" << sl << "_4, o" << sl << "_5, o" << sl
+        << "_6, o" << sl << "_7);\n";
+    }
+    for (int j = 0; j < 4; ++j) {
+      s << "      u64 ";
+      bool first = true;
+      for (auto& kv : outs) {
+        s << (first ? "" : ", ") << "r" << kv.second << "_" << j;
+        first = false;
+      }
+      if (outs.empty()) s << "unused_" << j;
+      s << ";\n      {\n";
+      emit_word(s, 'f', j);
+      for (auto& kv : outs) s << "      r" << kv.second << "_" << j << " = " << v(kv.first) << ";\n";
+      for (size_t q = 0; q < part.pops.size(); ++q)
+        s << "      pc" << q << " += __popcll(" << v(part.pops[q].first) << ");\n";
+      s << "      }\n";
+    }
+    for (auto& kv : outs) {
+      const std::string o = std::to_string(kv.second);
+      s << "      st4(A.out[" << o << "] + c, r" << o << "_0, r" << o << "_1, r" << o << "_2, r" << o << "_3);\n";
+    }
+    s << "      w += 4;\n    } else {\n      {\n";
+    emit_word(s, 's', 0);
+    emit_store_word(s);
+    s << "      }\n      ++w;\n    }\n  }\n";
+    s << "  }\n";   // active
+    for (size_t j = 0; j < part.pops.size(); ++j) {
+      s << "  {\n    unsigned long long t = pc" << j << ";\n"
+        << "    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(~0u, t, o);\n"
+        << "    if (lane == 0 && t) atomicAdd(A.slots + " << part.pops[j].second << ", t);\n  }\n";
+    }
+    s << "}\n";
+    return s.str();
+  }
+};
+
 // On-disk cache of compiled kernels, so that short-lived processes (the
 // bsim_cuda driver runs once per test case) do not recompile: directory
 // $BSZ_KERNEL_CACHE (or ~/.cache/bitstreamzoo_b200; "off" disables), files
@@ -777,9 +1167,11 @@ Compiled compile_source(const std::string& src, int block_threads, double* compi
 }
 
 // Splits a segment into parts: a node that reads a temporary through a right
-// shift, or through a left shift of 2048 bits or more, starts a later part,
-// and that temporary becomes an output of its own part.
-std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg, bool cut_adds) {
+// shift, or through a left shift of 64 * shl_cut_words bits or more (2048 in
+// the warp form, 64 in the thread-sequential form), starts a later part, and
+// that temporary becomes an output of its own part.
+std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg, bool cut_adds,
+                        int64_t shl_cut_words = 32) {
   std::map<int, int> level;
   std::set<int> computed(seg.order.begin(), seg.order.end());
   std::set<int> cut_src;
@@ -789,7 +1181,7 @@ std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg, bool
     for (int o : {x.a, x.b}) {
       if (o < 0 || !computed.count(o)) continue;
       int l = level[o];
-      bool cut = (x.op == NOp::Shr) || (x.op == NOp::Shl && x.k / 64 >= 32) ||
+      bool cut = (x.op == NOp::Shr) || (x.op == NOp::Shl && x.k / 64 >= shl_cut_words) ||
                  (cut_adds && nodes[o].op == NOp::Add);
       if (cut) {
         cut_src.insert(o);
@@ -887,6 +1279,7 @@ std::string graph_key(const std::vector<Node>& nodes, const std::vector<int>& or
   put(sc.min_blocks);
   put(sc.prefetch);
   put(sc.cut_adds);
+  put(sc.layout);
   return k;
 }
 
@@ -917,10 +1310,15 @@ PartKernel part_kernel(const std::vector<Node>& nodes, const Part& p, int64_t N,
     if (it != part_cache().end()) return it->second;
   }
   PartKernel pk;
-  Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
-  const std::string src = g.source();
-  pk.c = compile_source(src, sc.warps * 32, compile_ms);
-  pk.warm = g.warm;
+  if (sc.layout == 1) {
+    GenSeq g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0};
+    pk.c = compile_source(g.source(), sc.warps * 32, compile_ms);
+    pk.warm = g.warm;
+  } else {
+    Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
+    pk.c = compile_source(g.source(), sc.warps * 32, compile_ms);
+    pk.warm = g.warm;
+  }
   std::lock_guard<std::mutex> lk(g_part_mu);
   part_cache()[key] = pk;
   return pk;
@@ -935,7 +1333,7 @@ bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& s
     if (plan_cache().count(graph_key(nodes, seg.order, seg.inputs, seg.outputs, seg.pops, (N % 64) != 0, sc)))
       return true;
   }
-  std::vector<Part> parts = split(nodes, seg, sc.cut_adds != 0);
+  std::vector<Part> parts = split(nodes, seg, sc.cut_adds != 0, sc.layout == 1 ? 1 : 32);
   for (Part& p : parts) {
     if (p.order.empty() && p.pops.empty()) continue;
     if (p.inputs.size() > kMaxInputs) return false;
@@ -943,8 +1341,13 @@ bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& s
       std::lock_guard<std::mutex> lk(g_part_mu);
       if (part_cache().count(part_key(nodes, p, (N % 64) != 0, sc))) continue;
     }
-    Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
-    if (!is_compiled(g.source())) return false;
+    if (sc.layout == 1) {
+      GenSeq g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0};
+      if (!is_compiled(g.source())) return false;
+    } else {
+      Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
+      if (!is_compiled(g.source())) return false;
+    }
   }
   return true;
 }
@@ -954,7 +1357,14 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
                        unsigned long long* d_slots, double* compile_ms) {
   Device& dev = impl_->dev;
   const ExecOptions& opt = impl_->opt;
-  const Schedule& sc = opt.sched;
+  Schedule sc = opt.sched;
+  if (sc.layout == 1) {
+    // the thread-sequential form moves 32-byte sectors: every input must be
+    // 32-byte aligned (the library's own buffers are 256-byte aligned; a
+    // borrowed caller buffer may not be), else the segment takes the warp form
+    for (int n : seg.inputs)
+      if (nodes[n].buf && (reinterpret_cast<uintptr_t>(nodes[n].buf->p) & 31)) sc.layout = 0;
+  }
   using clk = std::chrono::steady_clock;
   auto ms_since = [](clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); };
   auto tp = clk::now();
@@ -967,7 +1377,7 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
   }
   if (!plan) {
     auto np = std::make_shared<SegPlan>();
-    for (Part& p : split(nodes, seg, sc.cut_adds != 0)) {
+    for (Part& p : split(nodes, seg, sc.cut_adds != 0, sc.layout == 1 ? 1 : 32)) {
       if (p.order.empty() && p.pops.empty()) continue;
       if (p.inputs.size() > kMaxInputs) throw RuntimeError("fused: too many inputs in one segment");
       np->kernels.push_back(part_kernel(nodes, p, N, sc, compile_ms));
@@ -994,19 +1404,34 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
       args[i] = x.buf ? reinterpret_cast<uint64_t>(x.buf->p) : 0;
     }
     for (size_t i = 0; i < p.outputs.size(); ++i) args[ni + i] = reinterpret_cast<uint64_t>(nodes[p.outputs[i]].buf->p);
-    // grid: contiguous ranges of whole 32-word steps, at least 8 warm-ups long
-    const int64_t steps = (nw + 31) / 32;
-    // persistent grid: as many warps as the compiled kernel keeps resident
+    int64_t range = 0;
+    int blocks = 1;
     const int per_sm = sc.ctas_per_sm > 0 ? std::min(sc.ctas_per_sm, c.blocks_per_sm) : c.blocks_per_sm;
-    // ctas_per_sm < 0: no persistent cap, every warp takes one range of the
-    // minimum length (more warps, shorter ranges, more warm-up work)
-    const int64_t max_warps = sc.ctas_per_sm < 0 ? std::numeric_limits<int64_t>::max() / 2
-                                                 : static_cast<int64_t>(dev.sm_count()) * per_sm * sc.warps;
-    int64_t min_range_steps = std::max<int64_t>(sc.range_steps, (pk.warm / 32) * 8);
-    int64_t warps_needed = std::max<int64_t>(1, std::min(max_warps, (steps + min_range_steps - 1) / min_range_steps));
-    int64_t range = ((steps + warps_needed - 1) / warps_needed) * 32;
-    int64_t total_warps = (nw + range - 1) / range;
-    int blocks = static_cast<int>((total_warps + sc.warps - 1) / sc.warps);
+    if (sc.layout == 1) {
+      // thread-sequential: one range of whole 4-word chunks per thread, at
+      // least 16 warm-ups long; a persistent grid of what stays resident
+      const int64_t threads_cap = sc.ctas_per_sm < 0 ? std::numeric_limits<int64_t>::max() / 2
+                                                     : static_cast<int64_t>(dev.sm_count()) * per_sm * sc.warps * 32;
+      const int64_t min_range = std::max<int64_t>(64, 16 * pk.warm);
+      int64_t threads = std::max<int64_t>(1, std::min(threads_cap, (nw + min_range - 1) / min_range));
+      range = ((nw + threads - 1) / threads + 3) / 4 * 4;
+      range = std::min<int64_t>(std::max<int64_t>(range, 4), int64_t(1) << 25);   // per-thread popcounts fit u32
+      const int64_t total = (nw + range - 1) / range;
+      blocks = static_cast<int>((total + sc.warps * 32 - 1) / (sc.warps * 32));
+    } else {
+      // grid: contiguous ranges of whole 32-word steps, at least 8 warm-ups long
+      const int64_t steps = (nw + 31) / 32;
+      // persistent grid: as many warps as the compiled kernel keeps resident;
+      // ctas_per_sm < 0: no persistent cap, every warp takes one range of the
+      // minimum length (more warps, shorter ranges, more warm-up work)
+      const int64_t max_warps = sc.ctas_per_sm < 0 ? std::numeric_limits<int64_t>::max() / 2
+                                                   : static_cast<int64_t>(dev.sm_count()) * per_sm * sc.warps;
+      int64_t min_range_steps = std::max<int64_t>(sc.range_steps, (pk.warm / 32) * 8);
+      int64_t warps_needed = std::max<int64_t>(1, std::min(max_warps, (steps + min_range_steps - 1) / min_range_steps));
+      range = ((steps + warps_needed - 1) / warps_needed) * 32;
+      int64_t total_warps = (nw + range - 1) / range;
+      blocks = static_cast<int>((total_warps + sc.warps - 1) / sc.warps);
+    }
     args[ni + no + 0] = reinterpret_cast<uint64_t>(d_slots);
     args[ni + no + 1] = reinterpret_cast<uint64_t>(impl_->d_fail);
     args[ni + no + 2] = static_cast<uint64_t>(nw);

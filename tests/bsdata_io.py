@@ -62,3 +62,44 @@ def write_bsdata(path, bitlength, inputs=None, params=None, input_arrays=None, c
         f.write(b"\0")
         for p in parts:
             f.write(p)
+
+
+def read_bsdata(path):
+    """Reads a .bsdata file into {"cases": [case, ...]}, each case a dict with
+    bitlength, params, inputs, input_arrays, expected, iterations, feedback;
+    streams as Python ints, arrays as {index: value} (the format of
+    benchmark/bsdata.py:196-270: _bin, _array_bin, _broadcast_pack markers)."""
+    with open(path, "rb") as f:
+        raw = f.read()
+    sep = raw.index(b"\0")
+    header = json.loads(raw[:sep].decode())
+    blob = memoryview(raw)[sep + 1:]
+
+    def value(v):
+        if isinstance(v, dict):
+            if "_bin" in v:
+                off, nb = v["_bin"]
+                return int.from_bytes(blob[off:off + nb], "little")
+            if "_array_bin" in v:
+                count, off, stride = v["_array_bin"]
+                return {i: int.from_bytes(blob[off + i * stride:off + (i + 1) * stride], "little")
+                        for i in range(count)}
+            if "_broadcast_pack" in v:
+                count, off, nb = v["_broadcast_pack"]
+                bits = int.from_bytes(blob[off:off + nb], "little")
+                return {i: (-1 if (bits >> i) & 1 else 0) for i in range(count)}
+            return {k: value(x) for k, x in v.items()}
+        if isinstance(v, list):
+            return {i: value(x) for i, x in enumerate(v)}
+        return v
+
+    def case(h):
+        return {"bitlength": h.get("bitlength", h.get("n_vectors", 0)),
+                "params": h.get("params", {}),
+                "inputs": {k: value(x) for k, x in h.get("inputs", {}).items()},
+                "input_arrays": {k: value(x) for k, x in h.get("input_arrays", {}).items()},
+                "expected": {k: value(x) for k, x in h.get("expected", {}).items()},
+                "iterations": h.get("iterations", 1), "feedback": h.get("feedback") or {}}
+
+    key = "cases" if "cases" in header else ("layers" if "layers" in header else None)
+    return {"cases": [case(h) for h in header[key]] if key else [case(header)]}

@@ -20,22 +20,26 @@ from oracle import cwords, pyoracle
 import progen
 
 
+# fused forms: warp ranges with lane = word, and thread-sequential ranges
+FORMS = [(bz.MODE_PLAIN, None), (bz.MODE_FUSED, {"layout": 0}), (bz.MODE_FUSED, {"layout": 1})]
+
+
 def run_both(ctx, src, nbits, inputs):
     prog = pyoracle.parse(src)
     ref_out, ref_pops = cwords.run_straight_line(prog, nbits, inputs)
     results = {}
-    for mode in (bz.MODE_PLAIN, bz.MODE_FUSED):
-        r = ctx.run(src, nbits, inputs, mode=mode)
+    for mode, sched in FORMS:
+        r = ctx.run(src, nbits, inputs, mode=mode, schedule=sched)
         for name, words in ref_out.items():
             got = r.stream(name)
             exp = words.copy()
             exp[-1] &= np.uint64(bz_mask(nbits))
             if not np.array_equal(got, exp):
                 bad = int(np.argmax(got != exp))
-                raise AssertionError(f"mode {mode} output {name}: first bad word {bad} of {got.size}")
+                raise AssertionError(f"mode {mode} {sched} output {name}: first bad word {bad} of {got.size}")
         for name, v in ref_pops.items():
-            assert r.int(name) == v, (mode, name)
-        results[mode] = r.stats
+            assert r.int(name) == v, (mode, sched, name)
+        results[(mode, (sched or {}).get("layout"))] = r.stats
     return results
 
 
@@ -49,7 +53,8 @@ def bz_mask(nbits):
 def test_long_streams(ctx, nbits):
     inputs = wl.long_streams_inputs(nbits, seed=nbits)
     st = run_both(ctx, wl.long_streams_src(), nbits, inputs)
-    assert st[bz.MODE_FUSED]["n_fused_launches"] >= 1
+    assert st[(bz.MODE_FUSED, 0)]["n_fused_launches"] >= 1
+    assert st[(bz.MODE_FUSED, 1)]["n_fused_launches"] >= 1
 
 
 @pytest.mark.gpu
@@ -89,7 +94,8 @@ def test_unresolvable_carry_falls_back_exactly(ctx):
     rng = np.random.default_rng(4)
     inputs = {"x": wl.random_words(rng, nbits), "z": wl.random_words(rng, nbits)}
     st = run_both(ctx, src, nbits, inputs)
-    assert st[bz.MODE_FUSED]["n_fused_fallbacks"] >= 1
+    assert st[(bz.MODE_FUSED, 0)]["n_fused_fallbacks"] >= 1
+    assert st[(bz.MODE_FUSED, 1)]["n_fused_fallbacks"] >= 1
 
 
 @pytest.mark.gpu
@@ -105,8 +111,8 @@ def test_random_straight_line_programs_fused_matches_plain_and_oracle(ctx):
         except Exception:
             continue
         mask = (1 << nbits) - 1
-        for mode in (bz.MODE_PLAIN, bz.MODE_FUSED):
-            r = ctx.run(src, nbits, inputs, meta["params"], arrays, mode=mode)
+        for mode, sched in FORMS:
+            r = ctx.run(src, nbits, inputs, meta["params"], arrays, mode=mode, schedule=sched)
             assert r.stream_int("out0") & mask == want["out0"] & mask, (seed, mode)
             assert r.stream_int("out1") & mask == want["out1"] & mask, (seed, mode)
             for j in range(3):
