@@ -58,6 +58,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-op comparison form")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's bsim_cuda")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="default run: skip the regex_dag and batched workloads (extra keys of the line)")
     ap.add_argument("--schedule", default="tuned", choices=["tuned", "model", "model1", "default"],
                     help="fused-kernel schedule: the autotuner's pick (every candidate of the 16-schedule "
                          "space timed before the timed region), the fastest of the shipped cost model's 4 "
@@ -130,7 +133,65 @@ def alu_roofline(prog, nbits: int, launch_ms: float, clocks) -> dict:
 
 
 DEFAULT_BITS = {"long_streams": 1 << 32, "regex_dag": 1 << 29, "matchstar": 1 << 24}
-DEFAULT_CPU_SAMPLE = {"long_streams": 1 << 28, "regex_dag": 1 << 26, "matchstar": 1 << 24}
+# CPU reference runs: the whole workload where it runs within seconds per pass
+# (long_streams: ~4-5 s at 2^32 bits on 16 threads); the 2,000-statement
+# regex DAG (the reference interpreter executes all of them, dead or not)
+# takes ~25 s per pass at 2^29 bits, so it is timed on a 2^26-bit sample.
+DEFAULT_CPU_SAMPLE = {"long_streams": 1 << 32, "regex_dag": 1 << 26, "matchstar": 1 << 24}
+
+
+def streams_as_locals(src: str, out_streams) -> str:
+    """The program with its output streams declared as local streams: the same
+    operations, with only the popcounts as outputs.  The reference executors
+    print every output stream as hex JSON (7 GB of text for long_streams at
+    2^32 bits), which would dwarf the computation being timed."""
+    keep = set(out_streams)
+    lines = []
+    for ln in src.splitlines():
+        t = ln.split()
+        if len(t) == 3 and t[:2] == ["output", "stream"] and t[2] in keep:
+            lines.append(f"stream {t[2]}")
+        else:
+            lines.append(ln)
+    return "\n".join(lines) + "\n"
+
+
+def reference_gpu(W, reps: int = 3):
+    """The reference's own GPU executor (bsim_cuda, built from its sources by
+    oracle/Makefile) on the same workload: one process per run, as the
+    harness runs it, on the program with its output streams as locals.  Its
+    JSON reports exec_ms (host wall time around interp.run: input H2D,
+    allocations, every kernel, result D2H) and timing.kernel_ms (CUDA events
+    around the same window).  Median of ``reps`` runs after one warm-up."""
+    from bitstreamzoo_b200.bsdata import write_bsdata
+    exe = os.path.join(ROOT, "oracle", "_ref", "bsim_cuda")
+    if not os.path.exists(exe):
+        return {"unavailable": "reference bsim_cuda not built (make -C oracle ref)"}
+    with tempfile.TemporaryDirectory() as td:
+        prog = os.path.join(td, f"{W.name}.bs")
+        with open(prog, "w") as f:
+            f.write(streams_as_locals(W.src, W.out_streams))
+        data = os.path.join(td, "in.bsdata")
+        write_bsdata(data, W.nbits, W.inputs)
+        env = dict(os.environ, GLIBC_TUNABLES="glibc.cpu.x86_rep_stosb_threshold=2000000000")
+        runs = []
+        for i in range(1 + reps):
+            r = subprocess.run([exe, prog, "--word-bits=64", "--reuse-mem", "--input", data],
+                               capture_output=True, text=True, env=env, timeout=900)
+            if r.returncode != 0:
+                return {"unavailable": "bsim_cuda failed: " + r.stderr.strip()[-200:]}
+            if i:
+                runs.append(json.loads(r.stdout))
+    exec_ms = statistics.median(o["exec_ms"] for o in runs)
+    kernel_ms = statistics.median(o["timing"]["kernel_ms"] for o in runs)
+    return {"impl": "bsim_cuda (reference, built from its sources for sm_100)", "exec_ms": exec_ms,
+            "kernel_ms": kernel_ms, "value": W.in_bytes / (kernel_ms * 1e-3) / 1e9, "unit": "GB/s",
+            "e2e_value": W.in_bytes / (exec_ms * 1e-3) / 1e9,
+            "n_kernel_launches": runs[0].get("n_kernel_launches"), "n_mallocs": runs[0].get("n_mallocs"),
+            "pops": {k: v for k, v in runs[0]["outputs"].items()}, "runs": reps,
+            "window": ("timing.kernel_ms: the reference's CUDA-event window around interp.run, which "
+                       "includes its input H2D copies and allocations; program with the output streams "
+                       "as locals (popcounts only)")}
 
 
 def peaks():
@@ -244,7 +305,7 @@ def cpu_baseline(workload: str, nbits: int, reps: int, warm: int = 1):
         with tempfile.TemporaryDirectory() as td:
             prog = os.path.join(td, f"{workload}.bs")
             with open(prog, "w") as f:
-                f.write(w.src)
+                f.write(streams_as_locals(w.src, w.out_streams))
             data = os.path.join(td, "in.bsdata")
             write_bsdata(data, nbits, w.inputs)
             env = dict(os.environ, OMP_NUM_THREADS=str(threads),
@@ -275,8 +336,9 @@ def cpu_baseline(workload: str, nbits: int, reps: int, warm: int = 1):
                 "single_core": {"value": w.in_bytes / (ms1 * 1e-3) / 1e9, "unit": "GB/s", "cores": 1,
                                 "backend": "bsim --backend simd", "ms": ms1},
                 "kind": "reference", "ms_per_step": ms,
-                "sample": (f"{workload} program at {nbits} bits per stream (1/{max(1, full // nbits)} "
-                           f"of the {full}-bit workload), bsim --backend simd_omp, "
+                "sample": (f"{workload} program at {nbits} bits per stream ("
+                           + ("the full workload" if nbits >= full else f"1/{full // nbits} of the {full}-bit workload")
+                           + f"; output streams as locals, popcounts out), bsim --backend simd_omp, "
                            f"OMP_NUM_THREADS={threads}, median exec_ms of {reps} runs")}
     from oracle import cwords, pyoracle
     prog = pyoracle.parse(w.src)
@@ -316,55 +378,77 @@ def run_reference(args, rank, world):
 
 # ---------------------------------------------------------------- GPU side --
 
-def run_ours(args, rank, world, local):
-    import torch
-    import bitstreamzoo_b200 as bz
-    from bitstreamzoo_b200 import workloads as wl
+class Env:
+    """Per-rank GPU context shared by the workloads one bench run measures."""
 
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    hbm, hbm_src = peaks()
-    nbits = args.nbits or DEFAULT_BITS[args.workload]
+    def __init__(self, args, rank, world, local):
+        import torch
+        import bitstreamzoo_b200 as bz
+        self.torch, self.bz = torch, bz
+        self.args, self.rank, self.world, self.local = args, rank, world, local
+        self.dist = None
+        if world > 1:
+            import torch.distributed as dist
+            from datetime import timedelta
+            dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+            self.dist = dist
+        torch.cuda.set_device(local)
+        self.dev = torch.device("cuda", local)
+        self.hbm, self.hbm_src = peaks()
+        self.ctx = bz.Context(local)
+        self.ext = torch.cuda.ExternalStream(self.ctx.stream, device=self.dev)
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+        self.torch.cuda.synchronize()
+
+    def max_over_ranks(self, x: float) -> float:
+        return reduce_max(x, self.dist, self.dev)
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def measure_workload(E, workload: str, nbits: int, steps: int, warmup: int, main_mode: str = "fused",
+                     with_plain: bool = True, with_e2e: bool = True, with_cpu: bool = True,
+                     with_ref_gpu: bool = True, schedule: str = "tuned", cpu_sample: int = 0):
+    """Measures one workload on this rank: the fused (and plain) form with
+    inputs resident in HBM, the end-to-end form through the C ABI, the
+    reference's GPU and CPU executors beside them (rank 0, one GPU).
+    Returns the bench line's fields for it."""
+    torch, bz = E.torch, E.bz
+    from bitstreamzoo_b200 import workloads as wl
+    args, rank, world, ctx = E.args, E.rank, E.world, E.ctx
     nw = wl.n_words(nbits)
-    W = Workload(args.workload, nbits, seed=20261204 + rank)
-    ctx = bz.Context(local)
-    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    W = Workload(workload, nbits, seed=20261204 + rank)
     prog = ctx.compile(W.src)
-    dev_in = {k: torch.from_numpy(v.view(np.int64)).to(dev) for k, v in W.inputs.items()}
+    dev_in = {k: torch.from_numpy(v.view(np.int64)).to(E.dev) for k, v in W.inputs.items()}
     torch.cuda.synchronize()
     mode_of = {"fused": bz.MODE_FUSED, "plain": bz.MODE_PLAIN}
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x: float) -> float:
-        return reduce_max(x, dist, dev)
-
     sched, sched_src = dict(bz.DEFAULT_SCHEDULE), "default"
-    if args.schedule == "tuned":
+    if schedule == "tuned":
         from bitstreamzoo_b200 import tuner
         ins = {k: (t.data_ptr(), nw) for k, t in dev_in.items()}
         sched = tuner.Autotuner(ctx).best(prog, W.src, nbits, ins)
         sched_src = (f"autotuner: fastest of all {len(tuner.CANDIDATES)} candidates "
                      "(median of 3 device-timed runs each, before the timed region)")
-    elif args.schedule in ("model", "model1"):
+    elif schedule in ("model", "model1"):
         from bitstreamzoo_b200 import tuner
         model = tuner.CostModel.load_default(ctx)
-        if model is not None and args.schedule == "model1":
+        if model is not None and schedule == "model1":
             sched, sched_src = model.choose(prog, nbits), "cost model top-1 (no timing)"
         elif model is not None:
             ins = {k: (t.data_ptr(), nw) for k, t in dev_in.items()}
             sched = model.choose(prog, nbits, top_k=4, inputs=ins)
             sched_src = "fastest of the cost model's top 4 (timed before the timed region)"
 
-    def step(mode):
+    outs_dev = {}
+
+    def step(mode, keep=False):
         r = prog.run(nbits, mode)
         if mode == bz.MODE_FUSED:
             r.set_schedule(sched)
@@ -372,61 +456,73 @@ def run_ours(args, rank, world, local):
             r.bind(k, ("borrow", t.data_ptr(), nw))
         st = r.execute()
         pops = {n: r.int(n) for n in W.out_ints}
+        if keep:
+            # device copies of the output streams, for the fused-vs-plain check
+            outs_dev[mode] = {}
+            bz._lib.check(r.lib.bsz_sync(ctx.h))
+            for n in W.out_streams:
+                outs_dev[mode][n] = _dev_view(r.stream_device_ptr(n), nw, E.dev).clone()
+            torch.cuda.synchronize()
         del r
         return st, pops
 
     forms = {}
-    order = [args.mode] + ([] if args.no_plain else [m for m in ("fused", "plain") if m != args.mode])
+    order = [main_mode] + ([m for m in ("fused", "plain") if m != main_mode] if with_plain else [])
     for name in order:
         mode = mode_of[name]
         try:
-            for _ in range(args.warmup):
-                st, pops = step(mode)
+            for i in range(warmup):
+                st, pops = step(mode, keep=(i == warmup - 1))
         except bz.BszError as e:
             forms[name] = {"unavailable": str(e)[:200]}
             continue
-        compile_ms = st.get("compile_ms", 0.0)
-        barrier()
+        E.barrier()
         ctx.profile(True)
-        clocks = Clocks(local)
+        clocks = Clocks(E.local)
         clocks.start()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(ext)
+        e0.record(E.ext)
         launches = fallbacks = 0
-        for _ in range(args.steps):
+        for _ in range(steps):
             st, pops = step(mode)
             launches += st["n_kernel_launches"]
             fallbacks += st["n_fused_fallbacks"]
-        e1.record(ext)
+        e1.record(E.ext)
         e1.synchronize()
-        barrier()
+        E.barrier()
         ms = e0.elapsed_time(e1)
         ck = clocks.stop()
         prof = ctx.profile_report()
         ctx.profile(False)
-        ms_max = max_over_ranks(ms)
+        ms_max = E.max_over_ranks(ms)
         forms[name] = {"ms": ms_max, "launches": launches, "fused_fallbacks": fallbacks,
                        "profile": prof, "clocks": ck, "pops": pops,
-                       "value": world * W.in_bytes * args.steps / (ms_max * 1e-3) / 1e9,
-                       "hbm_frac_step": ((W.in_bytes + W.out_bytes) * args.steps / (ms_max * 1e-3) / 1e9) / hbm}
+                       "value": world * W.in_bytes * steps / (ms_max * 1e-3) / 1e9,
+                       "hbm_frac_step": ((W.in_bytes + W.out_bytes) * steps / (ms_max * 1e-3) / 1e9) / E.hbm}
 
-    # cheap host checks of popcounts the two forms must agree on (and, for the
-    # long-stream workload, two that numpy computes exactly)
+    # parity inside the bench: the fused and the plain (per-op) forms are
+    # independent implementations; their output streams and popcounts must
+    # agree word for word (the full-size comparisons with the CPU oracle are
+    # the -m gpu tests)
+    check = {}
     if "pops" in forms.get("fused", {}) and "pops" in forms.get("plain", {}):
-        forms["fused"]["agrees_with_plain"] = forms["fused"]["pops"] == forms["plain"]["pops"]
-    if args.workload == "long_streams":
+        check["popcounts_fused_eq_plain"] = forms["fused"]["pops"] == forms["plain"]["pops"]
+        if bz.MODE_FUSED in outs_dev and bz.MODE_PLAIN in outs_dev:
+            check["streams_fused_eq_plain"] = all(
+                torch.equal(outs_dev[bz.MODE_FUSED][n], outs_dev[bz.MODE_PLAIN][n]) for n in W.out_streams)
+    if workload == "long_streams":
         ref_px = int(np.bitwise_count(W.inputs["A"] ^ W.inputs["B"]).sum())
         ref_pl64 = int(np.bitwise_count(W.inputs["A"][:-1]).sum())
-        for f in forms.values():
-            if "pops" in f:
-                f["check"] = (f["pops"]["px"] == ref_px and f["pops"]["pl64"] == ref_pl64)
+        check["numpy_px_pl64"] = all(f["pops"]["px"] == ref_px and f["pops"]["pl64"] == ref_pl64
+                                     for f in forms.values() if "pops" in f)
+    outs_dev.clear()
 
     # end to end through the C ABI: pinned host in, every output out
     e2e = None
-    main = forms.get(args.mode, {})
-    if not args.no_e2e and "ms" in main:
-        mode = mode_of[args.mode]
+    main = forms.get(main_mode, {})
+    if with_e2e and "ms" in main:
+        mode = mode_of[main_mode]
         pinned_in = {k: torch.from_numpy(v.view(np.int64)).pin_memory() for k, v in W.inputs.items()}
         pinned_out = {n: torch.empty(nw, dtype=torch.int64).pin_memory() for n in W.out_streams}
         in_np = {k: t.numpy().view(np.uint64) for k, t in pinned_in.items()}
@@ -434,6 +530,8 @@ def run_ours(args, rank, world, local):
 
         def e2e_step():
             r = prog.run(nbits, mode)
+            if mode == bz.MODE_FUSED:
+                r.set_schedule(sched)
             for k, a in in_np.items():
                 r.bind(k, a)
             r.execute()
@@ -443,99 +541,143 @@ def run_ours(args, rank, world, local):
             del r
             return vals
 
-        for _ in range(max(1, min(args.warmup, 2))):
+        for _ in range(max(1, min(warmup, 2))):
             e2e_step()
-        barrier()
-        k = max(1, min(args.steps, 5))
+        E.barrier()
+        k = max(1, min(steps, 5))
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
-        e0.record(ext)
+        e0.record(E.ext)
         for _ in range(k):
             e2e_step()
-        e1.record(ext)
+        e1.record(E.ext)
         e1.synchronize()
         wall = (time.perf_counter() - t0) * 1e3
-        barrier()
-        ms = max_over_ranks(max(e0.elapsed_time(e1), wall))
+        E.barrier()
+        ms = E.max_over_ranks(max(e0.elapsed_time(e1), wall))
         e2e = {"value": world * W.in_bytes * k / (ms * 1e-3) / 1e9, "unit": "GB/s",
-               "h2d_bytes_per_step": W.in_bytes, "d2h_bytes_per_step": len(W.out_streams) * nw * 8 + 8 * len(W.out_ints),
+               "h2d_bytes_per_step": W.in_bytes,
+               "d2h_bytes_per_step": len(W.out_streams) * nw * 8 + 8 * len(W.out_ints),
                "steps": k, "ms_per_step": ms / k}
+        del pinned_in, pinned_out
 
-    cb = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    cb = ref_gpu = None
+    if rank == 0 and world == 1:
+        if with_cpu:
+            try:
+                cb = cpu_baseline(workload, cpu_sample or DEFAULT_CPU_SAMPLE[workload], 5)
+            except Exception as e:  # noqa: BLE001
+                cb = {"unavailable": str(e)[:200]}
+        if with_ref_gpu:
+            try:
+                ref_gpu = reference_gpu(W)
+            except Exception as e:  # noqa: BLE001
+                ref_gpu = {"unavailable": str(e)[:200]}
+            if "pops" in ref_gpu and "pops" in main:
+                ref_gpu["agrees_with_ours"] = all(int(ref_gpu["pops"][n]) == main["pops"][n] for n in W.out_ints)
+                check["popcounts_eq_reference_bsim_cuda"] = ref_gpu["agrees_with_ours"]
+
+    prof = main.get("profile", {})
+    roof = None
+    if prof:
+        kname, kv = max(prof.items(), key=lambda kv: kv[1]["ms"])
+        per_launch_ms = kv["ms"] / max(1, kv["launches"])
+        bytes_launch = W.kernel_bytes(kname)
+        achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                traffic = json.load(f).get(f"{workload}:{kname}:layout{sched.get('layout', 0)}")
+        roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": E.hbm,
+                "peak_source": E.hbm_src, "unit": "GB/s", "frac": achieved / E.hbm,
+                "traffic": traffic, "bytes_per_launch": bytes_launch,
+                "launch_ms": per_launch_ms,
+                "kernel_share": kv["ms"] / max(1e-9, sum(x["ms"] for x in prof.values()))}
+        if kname.startswith("fused"):
+            roof["alu"] = alu_roofline(prog, nbits, per_launch_ms, main.get("clocks"))
+    res = {
+        "metric": metric_name(workload), "value": main.get("value"), "unit": "GB/s",
+        "ms_per_step": main.get("ms", float("nan")) / steps, "steps": steps, "warmup": warmup,
+        "data": W.data,
+        "config": {"workload": W.desc + " (per GPU)", "form": main_mode, "bits_per_stream": nbits,
+                   "schedule": sched, "schedule_source": sched_src,
+                   "l2": ("inputs larger than L2; no flush needed" if W.in_bytes > (126 << 20)
+                          else "inputs fit in L2 (reported, not roofline-judged)"),
+                   "parallelism": f"replicas x{world} (independent stream sets)"},
+        "hbm_frac_step": main.get("hbm_frac_step"), "roofline": roof, "cpu_baseline": cb, "e2e": e2e,
+        "gpu_launches": main.get("launches"), "clocks": main.get("clocks"), "check": check,
+        "forms": {k: {kk: vv for kk, vv in v.items() if kk != "pops"} for k, v in forms.items()},
+    }
+    if ref_gpu is not None:
+        res["forms"]["reference_gpu"] = {k: v for k, v in ref_gpu.items() if k != "pops"}
+        if "kernel_ms" in ref_gpu and "ms" in main:
+            res["vs_reference_gpu"] = {"device": ref_gpu["kernel_ms"] / (main["ms"] / steps),
+                                       "e2e": (ref_gpu["exec_ms"] / e2e["ms_per_step"]) if e2e else None}
+    del dev_in
+    torch.cuda.empty_cache()
+    return res
+
+
+def _dev_view(ptr: int, n: int, dev):
+    """A torch int64 tensor viewing n words of device memory at ptr (no copy)."""
+    import torch
+
+    class _Arr:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "<i8", "data": (ptr, False), "version": 3}
+    return torch.as_tensor(_Arr(), device=dev)
+
+
+def run_ours(args, rank, world, local):
+    E = Env(args, rank, world, local)
+    nbits = args.nbits or DEFAULT_BITS[args.workload]
+    res = measure_workload(E, args.workload, nbits, args.steps, args.warmup, main_mode=args.mode,
+                           with_plain=not args.no_plain, with_e2e=not args.no_e2e,
+                           with_cpu=not args.no_cpu_baseline, with_ref_gpu=not args.no_ref_gpu,
+                           schedule=args.schedule, cpu_sample=args.cpu_sample_bits)
+    extra = {}
+    if not args.no_extra and args.workload == "long_streams" and not args.nbits:
+        # the other benchmark workloads, as extra keys of the same line
         try:
-            cb = cpu_baseline(args.workload, args.cpu_sample_bits or DEFAULT_CPU_SAMPLE[args.workload], 5)
+            extra["regex_dag"] = measure_workload(E, "regex_dag", DEFAULT_BITS["regex_dag"], args.steps,
+                                                  args.warmup, with_e2e=False, schedule=args.schedule)
         except Exception as e:  # noqa: BLE001
-            cb = {"unavailable": str(e)[:200]}
-
+            extra["regex_dag"] = {"unavailable": str(e)[:300]}
+        try:
+            extra["batched"] = measure_batched(E, args.instances, args.steps, args.warmup)
+        except Exception as e:  # noqa: BLE001
+            extra["batched"] = {"unavailable": str(e)[:300]}
     if rank == 0:
-        prof = main.get("profile", {})
-        roof = None
-        if prof:
-            kname, kv = max(prof.items(), key=lambda kv: kv[1]["ms"])
-            per_launch_ms = kv["ms"] / max(1, kv["launches"])
-            bytes_launch = W.kernel_bytes(kname)
-            achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
-            traffic = None
-            tpath = os.path.join(ROOT, "profiles", "traffic.json")
-            if os.path.exists(tpath):
-                with open(tpath) as f:
-                    traffic = json.load(f).get(f"{args.workload}:{kname}")
-            roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
-                    "peak_source": hbm_src, "unit": "GB/s", "frac": achieved / hbm,
-                    "traffic": traffic, "bytes_per_launch": bytes_launch,
-                    "launch_ms": per_launch_ms,
-                    "kernel_share": kv["ms"] / max(1e-9, sum(x["ms"] for x in prof.values()))}
-            if kname.startswith("fused"):
-                roof["alu"] = alu_roofline(prog, nbits, per_launch_ms, main.get("clocks"))
-        line = {
-            "metric": metric_name(args.workload),
-            "value": main.get("value"), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": main.get("ms", float("nan")) / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
-            "data": W.data,
-            "config": {"workload": W.desc + " (per GPU)", "form": args.mode, "bits_per_stream": nbits,
-                       "schedule": sched, "schedule_source": sched_src,
-                       "l2": ("inputs larger than L2; no flush needed" if W.in_bytes > (126 << 20)
-                              else "inputs fit in L2 (reported, not roofline-judged)"),
-                       "parallelism": f"replicas x{world} (independent stream sets)"},
-            "hbm_frac_step": main.get("hbm_frac_step"),
-            "roofline": roof,
-            "cpu_baseline": cb,
-            "e2e": e2e,
-            "gpu_launches": main.get("launches"),
-            "clocks": main.get("clocks"),
-            "forms": {k: {kk: vv for kk, vv in v.items() if kk != "pops"} for k, v in forms.items()},
-        }
+        line = {"metric": res["metric"], "value": res["value"], "unit": "GB/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+                "data": res["data"], "config": res["config"], "hbm_frac_step": res["hbm_frac_step"],
+                "roofline": res["roofline"], "cpu_baseline": res["cpu_baseline"], "e2e": res["e2e"],
+                "gpu_launches": res["gpu_launches"], "clocks": res["clocks"], "check": res["check"],
+                "vs_reference_gpu": res.get("vs_reference_gpu"), "forms": res["forms"]}
+        if extra:
+            line["workloads"] = extra
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    E.close()
 
 
-def run_batched(args, rank, world, local):
+def measure_batched(E, instances: int, steps: int, warmup: int):
     """Batched uneven instances (one graph-captured persistent launch per
     step): 16 seeded 300-op regex-shaped DAGs, instance lengths log-uniform
     in [2^12, 2^26] bits, 8 inputs ~ Bernoulli(1/2) generated on the device,
-    4 outputs + 4 popcounts each.  value = input GB/s over all instances."""
-    import torch
-    import bitstreamzoo_b200 as bz
+    4 outputs + 4 popcounts each.  value = input GB/s over all instances.
+    Check: 64 instances' popcounts (the 16 longest among them) against their
+    own single-program runs in the plain per-op form (independent kernels);
+    the -m gpu tests compare instances with the CPU oracle."""
+    torch, bz = E.torch, E.bz
     from bitstreamzoo_b200 import workloads as wl
-
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    torch.cuda.set_device(local)
-    hbm, hbm_src = peaks()
-    srcs, plan = wl.batched_plan(n_instances=args.instances, n_dags=16, lo_log2=12, hi_log2=26, ops=300,
+    rank, world, ctx = E.rank, E.world, E.ctx
+    srcs, plan = wl.batched_plan(n_instances=instances, n_dags=16, lo_log2=12, hi_log2=26, ops=300,
                                  seed=20261207 + rank)
-    ctx = bz.Context(local)
     progs = [ctx.compile(s) for s in srcs]
     g = torch.Generator(device="cuda").manual_seed(20261208 + rank)
-    keep, instances = [], []
+    keep, insts = [], []
     in_bytes = out_bytes = 0
     for dag, bits in plan:
         nw = wl.n_words(bits)
@@ -547,73 +689,88 @@ def run_batched(args, rank, world, local):
                 t[-1:].bitwise_and_(m)
         dout = [torch.empty(nw, dtype=torch.int64, device="cuda") for _ in range(4)]
         keep += din + dout
-        instances.append((dag, bits, [t.data_ptr() for t in din], [t.data_ptr() for t in dout]))
+        insts.append((dag, bits, [t.data_ptr() for t in din], [t.data_ptr() for t in dout]))
         in_bytes += 8 * bits // 8
         out_bytes += 4 * bits // 8 + 4 * 8
     torch.cuda.synchronize()
     t0 = time.time()
-    b = bz.Batch(ctx, progs, instances)
+    b = bz.Batch(ctx, progs, insts)
     build_s = time.time() - t0
-    ext = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
-    for _ in range(max(3, args.warmup)):
+    for _ in range(max(3, warmup)):
         b.launch()
         b.finish()
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
+    E.barrier()
     ctx.profile(True)
-    clocks = Clocks(local)
+    clocks = Clocks(E.local)
     clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(ext)
-    for _ in range(args.steps):
+    e0.record(E.ext)
+    for _ in range(steps):
         b.launch()
-    e1.record(ext)
+    e1.record(E.ext)
     st = b.finish()
     e1.synchronize()
     ms = e0.elapsed_time(e1)
     ck = clocks.stop()
     prof = ctx.profile_report()
     ctx.profile(False)
-    ms = reduce_max(ms, dist, torch.device("cuda", local))
-    # spot check: a few instances against their own single-program runs (fused form)
-    rng = np.random.default_rng(rank)
-    check = True
-    for i in rng.choice(len(plan), size=min(6, len(plan)), replace=False):
-        dag, bits, ins, outs = instances[int(i)]
-        r = progs[dag].run(bits, bz.MODE_FUSED)
+    ms = E.max_over_ranks(ms)
+    # the 16 longest instances and 48 seeded others (the per-op form of all
+    # 4,096 would take minutes)
+    longest = sorted(range(len(plan)), key=lambda i: -plan[i][1])[:16]
+    rest = [i for i in np.random.default_rng(rank).permutation(len(plan)) if i not in set(longest)][:48]
+    n_check = 0
+    ok = True
+    for i in longest + [int(x) for x in rest]:
+        dag, bits, ins, outs = insts[i]
+        r = progs[dag].run(bits, bz.MODE_PLAIN)
         for j in range(8):
             r.bind(f"b{j}", ("borrow", ins[j], wl.n_words(bits)))
         r.execute()
-        check = check and [r.int(f"p{j}") for j in range(4)] == b.ints(int(i))
-    per_step = ms / args.steps
+        ok = ok and [r.int(f"p{j}") for j in range(4)] == b.ints(i)
+        n_check += 1
+        del r
+    per_step = ms / steps
     kname, kv = (max(prof.items(), key=lambda kv: kv[1]["ms"]) if prof else ("batch", {"ms": ms, "launches": 1}))
     launch_ms = kv["ms"] / max(1, kv["launches"])
     achieved = (in_bytes + out_bytes) / (launch_ms * 1e-3) / 1e9
-    if rank == 0:
-        line = {
-            "metric": "input GB/s (batched uneven instances, bit-exact)",
-            "value": world * in_bytes * args.steps / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": world,
-            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
-            "data": "synthetic (seeded: inputs ~ Bernoulli(1/2) generated on the device)",
-            "config": {"workload": f"batched: {len(plan)} instances of 16 seeded 300-op regex-shaped DAGs, "
-                                   "lengths log-uniform in [2^12, 2^26] bits, 8 inputs / 4 outputs + 4 popcounts each",
-                       "input_bytes": in_bytes, "output_bytes": out_bytes, "work_items": b.items,
-                       "build_s": build_s, "l2": "inputs (all instances) far larger than L2",
-                       "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
-                         "peak_source": hbm_src, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-                         "bytes_per_launch": in_bytes + out_bytes, "launch_ms": launch_ms},
-            "cpu_baseline": None, "e2e": None,
-            "gpu_launches": args.steps, "clocks": ck, "check": check, "fused_fallbacks": st.get("n_fused_fallbacks"),
-        }
-        print(json.dumps(line), flush=True)
+    res = {
+        "metric": "input GB/s (batched uneven instances, bit-exact)",
+        "value": world * in_bytes * steps / (ms * 1e-3) / 1e9, "unit": "GB/s",
+        "steps": steps, "warmup": max(3, warmup), "ms_per_step": per_step,
+        "data": "synthetic (seeded: inputs ~ Bernoulli(1/2) generated on the device)",
+        "config": {"workload": f"batched: {len(plan)} instances of 16 seeded 300-op regex-shaped DAGs, "
+                               "lengths log-uniform in [2^12, 2^26] bits, 8 inputs / 4 outputs + 4 popcounts each",
+                   "input_bytes": in_bytes, "output_bytes": out_bytes, "work_items": b.items,
+                   "build_s": build_s, "l2": "inputs (all instances) far larger than L2",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": E.hbm,
+                     "peak_source": E.hbm_src, "unit": "GB/s", "frac": achieved / E.hbm, "traffic": None,
+                     "bytes_per_launch": in_bytes + out_bytes, "launch_ms": launch_ms},
+        "cpu_baseline": {"unavailable": "the reference has no batched executor: its CPU path runs one "
+                                        "program per process"},
+        "e2e": None, "gpu_launches": steps, "clocks": ck,
+        "check": {"instances_checked": n_check, "popcounts_eq_plain_per_instance": ok},
+        "fused_fallbacks": st.get("n_fused_fallbacks"),
+    }
     del b
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    keep.clear()
+    torch.cuda.empty_cache()
+    return res
+
+
+def run_batched(args, rank, world, local):
+    E = Env(args, rank, world, local)
+    res = measure_batched(E, args.instances, args.steps, args.warmup)
+    if rank == 0:
+        line = {"metric": res["metric"], "value": res["value"], "unit": "GB/s", "n_gpus": world,
+                "steps": args.steps, "warmup": res["warmup"], "ms_per_step": res["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+                **{k: res[k] for k in ("data", "config", "roofline", "cpu_baseline", "e2e", "gpu_launches",
+                                        "clocks", "check", "fused_fallbacks")}}
+        print(json.dumps(line), flush=True)
+    E.close()
 
 
 def main():

@@ -66,12 +66,17 @@ def build(force: bool = False, verbose: bool = False) -> dict:
         mains = list(ex.map(lambda s: _compile(s, force, verbose), MAIN_SOURCES))
     so = os.path.join(LIB, "libbsz.so")
     # no -lcuda: driver entry points are resolved at run time (fused.cpp);
-    # the CUDA runtime is linked statically (the toolkit version it was built
-    # with), so whatever libcudart another library in the process loads does
-    # not matter.
-    link_libs = ["-L", os.path.join(CUDA_HOME, "lib64"), "-lnvrtc", "-cudart", "static"]
+    # the CUDA runtime and NVRTC are linked statically (the toolkit version
+    # this was built with), so whatever libcudart / libnvrtc another library
+    # in the process loads (PyTorch ships an older NVRTC, whose ptxas rejects
+    # the 256-bit loads and stores of the generated kernels) does not matter.
+    link_libs = ["-L", os.path.join(CUDA_HOME, "lib64"), "-lnvrtc_static", "-lnvrtc-builtins_static",
+                 "-lnvptxcompiler_static", "-cudart", "static", "-lpthread", "-ldl", "-lrt"]
     if force or _newer(so, objs):
+        # -Bsymbolic + --exclude-libs: the library's calls into its static
+        # NVRTC bind to its own copy and none of those symbols is exported
         cmd = [NVCC, *ARCH, "-shared", "-o", so, *objs, *link_libs,
+               "-Xlinker", "-Bsymbolic", "-Xlinker", "--exclude-libs,ALL",
                "-Xlinker", "-rpath", "-Xlinker", os.path.join(CUDA_HOME, "lib64")]
         if verbose:
             print(" ".join(cmd))
