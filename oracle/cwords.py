@@ -167,16 +167,81 @@ def program_to_ops(prog):
     return ops, {n: regs[n] for n in prog["inputs"]}, outs, pops, nxt[0], tails
 
 
+def compact_registers(ops, in_regs, out_regs, nregs):
+    """Drops the ops no output or popcount depends on and renumbers the
+    registers (written once each) so that a register's buffer is reused after
+    its last read: the register file then holds the peak number of live
+    values instead of one buffer per op.  A destination never shares a buffer
+    with an operand of its own op.
+    Returns (ops, in_regs, out_regs, n_physical)."""
+    def reads(o):
+        code, d, a, b, _ = o
+        r = [a] if a >= 0 else []
+        if b >= 0 and code != OP[">>"]:
+            r.append(b)
+        return r
+
+    # drop ops whose value reaches no output and no popcount
+    needed = set(out_regs.values())
+    keep = [False] * len(ops)
+    for j in range(len(ops) - 1, -1, -1):
+        o = ops[j]
+        if o[0] == OP["pop"] or o[1] in needed:
+            keep[j] = True
+            needed.update(reads(o))
+    ops = [o for o, k in zip(ops, keep) if k]
+    last = {}
+    for j, o in enumerate(ops):
+        for r in reads(o):
+            last[r] = j
+    # outputs live to the end; inputs are the caller's arrays (never reused)
+    pinned = set(out_regs.values()) | set(in_regs.values())
+    phys = {}
+    free = []
+    nphys = 0
+
+    def alloc():
+        nonlocal nphys
+        if free:
+            return free.pop()
+        nphys += 1
+        return nphys - 1
+
+    for r in in_regs.values():
+        phys[r] = alloc()
+    out_ops = []
+    for j, o in enumerate(ops):
+        code, d, a, b, imm = o
+        pa = phys[a] if a >= 0 else -1
+        pb = phys[b] if (b >= 0 and code != OP[">>"]) else b
+        if code == OP["pop"]:
+            out_ops.append((code, pa, pa, -1, imm))
+        else:
+            phys[d] = alloc()
+            out_ops.append((code, phys[d], pa, pb, imm))
+        for r in set(reads(o)):
+            if last.get(r) == j and r not in pinned:
+                free.append(phys[r])
+        if code != OP["pop"] and d not in last and d not in pinned:
+            free.append(phys[d])   # never read: its buffer is free right away
+    return (out_ops, {k: phys[r] for k, r in in_regs.items()}, {k: phys[r] for k, r in out_regs.items()},
+            max(1, nphys))
+
+
 def run_straight_line(prog, nbits, inputs: dict, reuse_inputs=False):
     """Evaluate a straight-line program with the C oracle.
 
     ``inputs`` maps names to numpy uint64 arrays (n words each).
     Returns (outputs dict name->array, popcounts dict name->int).
+    Registers are reused after their last read, so the memory held is the
+    peak number of live values times the stream size.
     """
     ops, in_regs, out_regs, pops, nregs, _ = program_to_ops(prog)
+    ops, in_regs, out_regs, nregs = compact_registers(ops, in_regs, out_regs, nregs)
     n = n_words(nbits)
     bufs = [None] * nregs
     for name, r in in_regs.items():
+        # inputs are never written (every op writes a fresh register)
         bufs[r] = np.ascontiguousarray(inputs[name], dtype=np.uint64)
     for r in range(nregs):
         if bufs[r] is None:

@@ -56,3 +56,16 @@ def test_s2p_small_against_reference_loop(ctx):
 def test_s2p_zero_bytes_is_a_no_op(ctx):
     ctx.s2p(0, 0, [0] * 8)
     ctx.sync()
+
+
+def test_s2p_matches_reference_goldens(ctx):
+    """bsz_s2p against the reference's own payload_to_basis_bits outputs."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "s2p_golden.json")) as f:
+        cases = json.load(f)["cases"]
+    for c in cases:
+        payload = np.frombuffer(bytes.fromhex(c["payload"]), dtype=np.uint8)
+        got = _run_s2p(ctx, payload)
+        want = [int(h, 16) for h in c["basis"]]
+        assert [int.from_bytes(w.astype("<u8").tobytes(), "little") for w in got] == want, c["name"]

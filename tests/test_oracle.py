@@ -7,6 +7,7 @@
 * the word-level C oracle against the same golden vectors.
 """
 
+import os
 import random
 
 import numpy as np
@@ -167,3 +168,21 @@ def test_basis_restatements_agree():
         for i in range(8):
             assert cwords.words_to_int(words[i]) == ints[i]
             assert words[i].size == (n + 63) // 64
+
+
+def test_basis_oracle_matches_reference_s2p_goldens():
+    """oracle/basis.py against payload_to_basis_bits(_fast) of the reference
+    (benchmark/apps/regex/src/run.py:164-187), via tests/golden/s2p_golden.json."""
+    import json
+    from oracle import basis
+    with open(os.path.join(os.path.dirname(__file__), "golden", "s2p_golden.json")) as f:
+        cases = json.load(f)["cases"]
+    assert len(cases) >= 20
+    for c in cases:
+        payload = bytes.fromhex(c["payload"])
+        want = [int(h, 16) for h in c["basis"]]
+        words = basis.basis_words(payload)
+        got = [int.from_bytes(w.astype("<u8").tobytes(), "little") for w in words]
+        assert got == want, c["name"]
+        if len(payload) <= 4096:
+            assert basis.basis_ints(payload) == want, c["name"]
