@@ -218,6 +218,7 @@ int bsz_run_set_schedule(bsz_run* run, const bsz_schedule* s) {
     c.prefetch = s->prefetch;
     c.cut_adds = s->cut_adds;
     c.layout = s->layout;
+    c.chunk_words = s->chunk_words;
     executor(run).set_schedule(c);
   });
 }

@@ -62,6 +62,8 @@ struct Schedule {
   int prefetch = 1;       // issue the next step's loads before the current step's arithmetic
   int cut_adds = 0;       // 1: every addition ends a part (its result is materialized)
   int layout = 0;         // 0: warp ranges, lane = word; 1: thread-sequential ranges
+                          // (register chunks); 2: thread-sequential ranges through TMA boxes
+  int chunk_words = 8;    // layout 2: words per thread per box (4 or 8)
 };
 
 struct ExecOptions {

@@ -58,6 +58,10 @@ struct Driver {
                             unsigned, CUstream, void**, void**) = nullptr;
   CUresult (*get_error_string)(CUresult, const char**) = nullptr;
   CUresult (*occupancy)(int*, CUfunction, int, size_t) = nullptr;
+  CUresult (*func_set_attribute)(CUfunction, CUfunction_attribute, int) = nullptr;
+  CUresult (*tensor_map_encode_tiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                      const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill) = nullptr;
 };
 
 template <class F>
@@ -79,6 +83,8 @@ const Driver& drv() {
     resolve("cuLaunchKernel", x.launch_kernel);
     resolve("cuGetErrorString", x.get_error_string);
     resolve("cuOccupancyMaxActiveBlocksPerMultiprocessor", x.occupancy);
+    resolve("cuFuncSetAttribute", x.func_set_attribute);
+    resolve("cuTensorMapEncodeTiled", x.tensor_map_encode_tiled);
     return x;
   }();
   return d;
@@ -135,7 +141,8 @@ void FusedBackend::set_schedule(const Schedule& s) {
   c.range_steps = std::max(1, c.range_steps);
   c.ctas_per_sm = std::max(-1, c.ctas_per_sm);
   c.min_blocks = std::max(1, std::min(c.min_blocks, 32));
-  c.layout = c.layout ? 1 : 0;
+  c.layout = std::max(0, std::min(c.layout, 2));
+  c.chunk_words = c.chunk_words == 4 ? 4 : 8;
   impl_->opt.sched = c;
 }
 
@@ -683,6 +690,13 @@ struct GenSeq {
   std::map<std::pair<int, int64_t>, int> off_slot;
   int64_t fast_lo = 0;               // a chunk at c is fast if c >= fast_lo ...
   int64_t fast_hi_pad = 3;           // ... and c + fast_hi_pad <= nw - 1 - masked
+  // TMA form (layout 2): inputs arrive as tensor-map boxes of `roww` words x
+  // 32 threads per warp in `stages` shared-memory stages, outputs leave the
+  // same way; shifted-input reads by 64 bits or more use bounded loads.
+  bool tma = false;
+  int roww = 8;
+  int stages = 2;
+  std::vector<int> mapped;           // input indices (A.in order) that are read through boxes
 
   std::string v(int n) const { return "v" + std::to_string(n); }
 
@@ -828,6 +842,7 @@ struct GenSeq {
     };
     auto word_at = [&](int n, int64_t off) -> std::string {
       if (slow) return ld(n, "w + (" + std::to_string(off) + "ll)");
+      if (tma) return ld(n, W + " + (" + std::to_string(off) + "ll)");
       return fast_off(n, off, j);
     };
     for (int n : emit_order) {
@@ -906,8 +921,158 @@ struct GenSeq {
     for (size_t j = 0; j < part.pops.size(); ++j) s << "      pc" << j << " += __popcll(" << v(part.pops[j].first) << ");\n";
   }
 
+  // Mapped inputs: every non-constant input of the part (in A.in order).
+  void compute_mapped() {
+    mapped.clear();
+    for (auto& kv : in_idx)
+      if (!is_const(nodes[kv.first].op)) mapped.push_back(kv.second);
+    std::sort(mapped.begin(), mapped.end());
+  }
+  int box_bytes() const { return roww * 8 * 32; }
+  // shared memory per warp: `stages` boxes per mapped input + one per output
+  int smem_per_warp() const {
+    return (stages * static_cast<int>(mapped.size()) + static_cast<int>(outs.size())) * box_bytes();
+  }
+  int smem_bytes() const { return warps * smem_per_warp() + 1024; }
+
+  // Argument block of the TMA form: the tensor maps (128 bytes, 64-byte
+  // aligned, one per mapped input then one per output) followed by the
+  // plain form's fields and the number of threads whose ranges the maps cover.
+  std::string tma_prelude(int ni, int no) const {
+    std::ostringstream s;
+    s << "struct __align__(64) TMap { unsigned long long w[16]; };\n"
+      << "struct ArgsT {\n  TMap in_map[" << std::max<size_t>(1, mapped.size()) << "];\n  TMap out_map["
+      << std::max(1, no) << "];\n  const u64* in[" << std::max(1, ni) << "];\n  u64* out[" << std::max(1, no)
+      << "];\n  unsigned long long* slots;\n  unsigned int* fail;\n  long long nw;\n  long long range;\n"
+      << "  u64 last_mask;\n  long long nfull;\n};\n"
+      << "__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }\n";
+    return s.str();
+  }
+
+  // The owned range through TMA boxes (see the struct comment).  All lanes of
+  // a warp walk the chunks together; lanes whose rows lie past the maps'
+  // rows (the one thread with a short range, and idle threads) skip the
+  // arithmetic, and the short range is done afterwards by the scalar path.
+  void emit_tma_body(std::ostringstream& s) const {
+    const int nm = static_cast<int>(mapped.size()), no = static_cast<int>(outs.size());
+    const int box = box_bytes(), rowb = roww * 8;
+    const std::string sw = roww == 4 ? "((lane >> 2) & 1)" : roww == 8 ? "((lane >> 1) & 3)" : "(lane & 7)";
+    s << "  extern __shared__ __align__(1024) unsigned char smraw[];\n"
+      << "  __shared__ __align__(8) unsigned long long bar[" << warps << "][" << stages << "];\n"
+      << "  const int warp = threadIdx.x >> 5;\n"
+      << "  unsigned char* sm = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);\n"
+      << "  unsigned char* wb = sm + warp * " << smem_per_warp() << ";\n"
+      << "  const long long t0 = tid - lane;\n"
+      << "  const bool full = tid < A.nfull;\n"
+      << "  const int sw = " << sw << ";\n"
+      << "  if (t0 < A.nfull) {\n"
+      << "    if (lane == 0) {\n"
+      << "      for (int q = 0; q < " << stages << "; ++q) asm volatile(\"mbarrier.init.shared.b64 [%0], 1;\" :: \"r\"(smem_u32(&bar[warp][q])));\n"
+      << "      asm volatile(\"fence.mbarrier_init.release.cluster;\" ::: \"memory\");\n"
+      << "    }\n    __syncwarp();\n"
+      << "    const int nch = (int)(A.range / " << roww << ");\n"
+      << "    auto issue = [&](int ch, int q) {\n"
+      << "      asm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n"
+      << "      __syncwarp();\n"
+      << "      if (lane == 0) {\n"
+      << "        const unsigned mb = smem_u32(&bar[warp][q]);\n"
+      << "        asm volatile(\"mbarrier.arrive.expect_tx.shared.b64 _, [%0], %1;\" :: \"r\"(mb), \"r\"(" << nm * box
+      << ") : \"memory\");\n";
+    for (int k = 0; k < nm; ++k)
+      s << "        asm volatile(\"cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+           "[%0], [%1, {%2, %3, %4}], [%5];\" :: \"r\"(smem_u32(wb + (q * "
+        << nm << " + " << k << ") * " << box << ")), \"l\"(&A.in_map[" << k
+        << "]), \"r\"(0), \"r\"(ch), \"r\"((int)t0), \"r\"(mb) : \"memory\");\n";
+    s << "      }\n    };\n"
+      << "    int issued = 0;\n"
+      << "    for (; issued < " << stages - 1 << " && issued < nch; ++issued) issue(issued, issued % " << stages << ");\n"
+      << "    unsigned phase = 0;\n    bool bail = false;\n    int waited = 0;\n"
+      << "    for (int ch = 0; ch < nch && !bail; ++ch) {\n"
+      << "      const int q = ch % " << stages << ";\n"
+      << "      if (issued < nch) { issue(issued, issued % " << stages << "); ++issued; }\n"
+      // bounded wait; a stage that never lands sets the fail flag (the host
+      // then re-runs the part with the exact per-op kernels)
+      << "      {\n        const unsigned mb = smem_u32(&bar[warp][q]);\n        unsigned done = 0;\n"
+      << "        for (int it = 0; it < (1 << 22) && !done; ++it)\n"
+      << "          asm volatile(\"{ .reg .pred p; mbarrier.try_wait.parity.shared.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }\" "
+         ": \"=r\"(done) : \"r\"(mb), \"r\"((phase >> q) & 1u) : \"memory\");\n"
+      << "        if (!__all_sync(~0u, done)) { if (lane == 0) atomicOr(A.fail, 2u); bail = true; break; }\n"
+      << "        phase ^= 1u << q;\n        ++waited;\n      }\n"
+      << "      if (lane == 0) asm volatile(\"cp.async.bulk.wait_group.read 0;\" ::: \"memory\");\n"
+      << "      __syncwarp();\n"
+      << "      const long long w0 = s + (long long)ch * " << roww << ";\n"
+      << "      unsigned char* ib = wb + q * " << nm * box << " + lane * " << rowb << ";\n"
+      << "      unsigned char* ob = wb + " << stages * nm * box << " + lane * " << rowb << ";\n"
+      << "      if (full) {\n"
+      << "        if (" << (masked ? "w0 + " + std::to_string(roww) + " <= A.nw - 1" : std::string("true")) << ") {\n"
+      << "#pragma unroll 1\n"
+      << "          for (int pp = 0; pp < " << roww / 2 << "; ++pp) {\n"
+      << "            const long long c = w0 + 2 * pp;\n"
+      << "            const int po = (pp ^ sw) * 16;\n";
+    for (int k = 0; k < nm; ++k) {
+      const std::string i = std::to_string(mapped[k]);
+      s << "            const ulonglong2 q" << i << " = *reinterpret_cast<const ulonglong2*>(ib + " << k * box
+        << " + po);\n            const u64 c" << i << "_0 = q" << i << ".x, c" << i << "_1 = q" << i << ".y;\n";
+    }
+    for (int j = 0; j < 2; ++j) {
+      s << "            u64 ";
+      bool first = true;
+      for (auto& kv : outs) {
+        s << (first ? "" : ", ") << "r" << kv.second << "_" << j;
+        first = false;
+      }
+      if (outs.empty()) s << "unused_" << j;
+      s << ";\n            {\n";
+      emit_word(s, 'f', j);
+      for (auto& kv : outs) s << "      r" << kv.second << "_" << j << " = " << v(kv.first) << ";\n";
+      for (size_t qq = 0; qq < part.pops.size(); ++qq)
+        s << "      pc" << qq << " += __popcll(" << v(part.pops[qq].first) << ");\n";
+      s << "            }\n";
+    }
+    for (auto& kv : outs)
+      s << "            *reinterpret_cast<ulonglong2*>(ob + " << kv.second * box << " + po) = make_ulonglong2(r"
+        << kv.second << "_0, r" << kv.second << "_1);\n";
+    s << "          }\n        } else {\n"
+      << "          for (long long w = w0; w < w0 + " << roww << "; ++w) {\n"
+      << "            const int jj = (int)(w - w0);\n"
+      << "            const int wo = ((jj >> 1) ^ sw) * 16 + (jj & 1) * 8;\n"
+      << "            {\n";
+    emit_word(s, 's', 0);
+    for (auto& kv : outs)
+      s << "      *reinterpret_cast<u64*>(ob + " << kv.second * box << " + wo) = " << v(kv.first) << ";\n";
+    for (size_t qq = 0; qq < part.pops.size(); ++qq)
+      s << "      pc" << qq << " += __popcll(" << v(part.pops[qq].first) << ");\n";
+    s << "            }\n          }\n        }\n      }\n"
+      << "      asm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n"
+      << "      __syncwarp();\n"
+      << "      if (lane == 0) {\n";
+    for (int o = 0; o < no; ++o)
+      s << "        asm volatile(\"cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];\" "
+           ":: \"l\"(&A.out_map[" << o << "]), \"r\"(0), \"r\"(ch), \"r\"((int)t0), \"r\"(smem_u32(wb + "
+        << stages * nm * box + o * box << ")) : \"memory\");\n";
+    s << "        asm volatile(\"cp.async.bulk.commit_group;\" ::: \"memory\");\n"
+      << "      }\n      __syncwarp();\n    }\n"
+      // after a bail-out: wait (bounded) for the loads still in flight
+      << "    if (bail) {\n"
+      << "      for (int ch = waited; ch < issued; ++ch) {\n"
+      << "        const int q = ch % " << stages << ";\n        const unsigned mb = smem_u32(&bar[warp][q]);\n"
+      << "        unsigned done = 0;\n"
+      << "        for (int it = 0; it < (1 << 22) && !done; ++it)\n"
+      << "          asm volatile(\"{ .reg .pred p; mbarrier.test_wait.parity.shared.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }\" "
+         ": \"=r\"(done) : \"r\"(mb), \"r\"((phase >> q) & 1u) : \"memory\");\n"
+      << "        phase ^= 1u << q;\n      }\n    }\n"
+      << "    if (lane == 0) asm volatile(\"cp.async.bulk.wait_group 0;\" ::: \"memory\");\n"
+      << "  }\n"
+      // the range past the maps' rows: scalar path, stores to global
+      << "  if (active && !full) {\n    for (long long w = s; w < e; ++w) {\n      {\n";
+    emit_word(s, 's', 0);
+    emit_store_word(s);
+    s << "      }\n    }\n  }\n";
+  }
+
   std::string source() {
     analyze();
+    compute_mapped();
     std::ostringstream s;
     const int ni = static_cast<int>(part.inputs.size()), no = static_cast<int>(part.outputs.size());
     s << Gen::args_struct(ni, no);
@@ -936,10 +1101,17 @@ struct GenSeq {
          "  asm volatile(\"ld.global.nc.L2::128B.v4.u64 {%0,%1,%2,%3}, [%4];\" : \"=l\"(a), \"=l\"(b), \"=l\"(c), \"=l\"(d) : \"l\"(p));\n}\n"
          "__device__ __forceinline__ void st4(u64* p, u64 a, u64 b, u64 c, u64 d) {\n"
          "  asm volatile(\"st.global.v4.u64 [%0], {%1,%2,%3,%4};\" :: \"l\"(p), \"l\"(a), \"l\"(b), \"l\"(c), \"l\"(d) : \"memory\");\n}\n";
-    s << "extern \"C\" __global__ void __launch_bounds__(" << warps * 32 << ", " << min_blocks
-      << ")\nbsz_fused(const Args A) {\n"
-      << "  const int lane = threadIdx.x & 31;\n"
-      << "  const long long s = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * A.range;\n"
+    if (tma) {
+      s << tma_prelude(ni, no);
+      s << "extern \"C\" __global__ void __launch_bounds__(" << warps * 32 << ", 1)\n"
+        << "bsz_fused(const __grid_constant__ ArgsT A) {\n";
+    } else {
+      s << "extern \"C\" __global__ void __launch_bounds__(" << warps * 32 << ", " << min_blocks
+        << ")\nbsz_fused(const Args A) {\n";
+    }
+    s << "  const int lane = threadIdx.x & 31;\n"
+      << "  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
+      << "  const long long s = tid * A.range;\n"
       << "  const bool active = s < A.nw;\n"
       << "  const long long e = min(s + A.range, A.nw);\n";
     std::vector<int> adds;
@@ -974,6 +1146,10 @@ struct GenSeq {
         << "    p0 = s - 2 * (s - p0);\n    if (p0 < 0) p0 = 0;\n"
         << "  }\n";
     }
+    if (tma) {
+      s << "  }\n";   // active (warm-up)
+      emit_tma_body(s);
+    } else {
     // ---- owned range
     const int pad = static_cast<int>(fast_hi_pad) + (masked && fast_hi_pad == 3 ? 1 : 0);
     s << "  long long w = s;\n"
@@ -1022,6 +1198,7 @@ struct GenSeq {
     emit_store_word(s);
     s << "      }\n      ++w;\n    }\n  }\n";
     s << "  }\n";   // active
+    }
     for (size_t j = 0; j < part.pops.size(); ++j) {
       s << "  {\n    unsigned long long t = pc" << j << ";\n"
         << "    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(~0u, t, o);\n"
@@ -1239,6 +1416,12 @@ namespace {
 struct PartKernel {
   Compiled c;
   int64_t warm = 0;
+  // TMA form: chunk words, dynamic shared memory, resident CTAs per SM at
+  // that size, and the A.in indices read through tensor maps (in map order)
+  int roww = 0;
+  int smem = 0;
+  int tma_blocks_per_sm = 0;
+  std::vector<int> mapped;
 };
 std::mutex g_part_mu;
 std::unordered_map<std::string, PartKernel>& part_cache() {
@@ -1280,6 +1463,7 @@ std::string graph_key(const std::vector<Node>& nodes, const std::vector<int>& or
   put(sc.prefetch);
   put(sc.cut_adds);
   put(sc.layout);
+  put(sc.chunk_words);
   return k;
 }
 
@@ -1310,7 +1494,32 @@ PartKernel part_kernel(const std::vector<Node>& nodes, const Part& p, int64_t N,
     if (it != part_cache().end()) return it->second;
   }
   PartKernel pk;
-  if (sc.layout == 1) {
+  // the TMA form's argument block holds a 128-byte tensor map per read input
+  // and per output; past 24 of them the part takes the register form
+  int n_maps = static_cast<int>(p.outputs.size());
+  for (int n : p.inputs)
+    if (!is_const(nodes[n].op)) ++n_maps;
+  if (sc.layout == 2 && n_maps > 24) {
+    Schedule s1 = sc;
+    s1.layout = 1;
+    s1.min_blocks = 1;
+    return part_kernel(nodes, p, N, s1, compile_ms);
+  }
+  if (sc.layout == 2) {
+    GenSeq g{nodes, p, N, sc.warps, 1, (N % 64) != 0};
+    g.tma = true;
+    g.roww = sc.chunk_words == 4 ? 4 : 8;
+    const std::string src = g.source();
+    pk.c = compile_source(src, sc.warps * 32, compile_ms);
+    pk.warm = g.warm;
+    pk.roww = g.roww;
+    pk.smem = g.smem_bytes();
+    pk.mapped = g.mapped;
+    BSZ_CU(drv().func_set_attribute(pk.c.fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, pk.smem));
+    if (drv().occupancy(&pk.tma_blocks_per_sm, pk.c.fn, sc.warps * 32, pk.smem) != CUDA_SUCCESS ||
+        pk.tma_blocks_per_sm < 1)
+      throw RuntimeError("fused: the TMA form does not fit on an SM (" + std::to_string(pk.smem) + " bytes)");
+  } else if (sc.layout == 1) {
     GenSeq g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0};
     pk.c = compile_source(g.source(), sc.warps * 32, compile_ms);
     pk.warm = g.warm;
@@ -1333,7 +1542,7 @@ bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& s
     if (plan_cache().count(graph_key(nodes, seg.order, seg.inputs, seg.outputs, seg.pops, (N % 64) != 0, sc)))
       return true;
   }
-  std::vector<Part> parts = split(nodes, seg, sc.cut_adds != 0, sc.layout == 1 ? 1 : 32);
+  std::vector<Part> parts = split(nodes, seg, sc.cut_adds != 0, sc.layout >= 1 ? 1 : 32);
   for (Part& p : parts) {
     if (p.order.empty() && p.pops.empty()) continue;
     if (p.inputs.size() > kMaxInputs) return false;
@@ -1341,7 +1550,12 @@ bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& s
       std::lock_guard<std::mutex> lk(g_part_mu);
       if (part_cache().count(part_key(nodes, p, (N % 64) != 0, sc))) continue;
     }
-    if (sc.layout == 1) {
+    if (sc.layout == 2) {
+      GenSeq g{nodes, p, N, sc.warps, 1, (N % 64) != 0};
+      g.tma = true;
+      g.roww = sc.chunk_words == 4 ? 4 : 8;
+      if (!is_compiled(g.source())) return false;
+    } else if (sc.layout == 1) {
       GenSeq g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0};
       if (!is_compiled(g.source())) return false;
     } else {
@@ -1358,13 +1572,16 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
   Device& dev = impl_->dev;
   const ExecOptions& opt = impl_->opt;
   Schedule sc = opt.sched;
-  if (sc.layout == 1) {
-    // the thread-sequential form moves 32-byte sectors: every input must be
+  if (sc.layout >= 1) {
+    // the thread-sequential forms move 32-byte sectors: every input must be
     // 32-byte aligned (the library's own buffers are 256-byte aligned; a
     // borrowed caller buffer may not be), else the segment takes the warp form
     for (int n : seg.inputs)
       if (nodes[n].buf && (reinterpret_cast<uintptr_t>(nodes[n].buf->p) & 31)) sc.layout = 0;
   }
+  // the TMA form pays off on long streams only (its boxes cover 32 threads'
+  // ranges); short ones take the register form
+  if (sc.layout == 2 && nw < (int64_t(1) << 16)) sc.layout = 1;
   using clk = std::chrono::steady_clock;
   auto ms_since = [](clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); };
   auto tp = clk::now();
@@ -1377,7 +1594,7 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
   }
   if (!plan) {
     auto np = std::make_shared<SegPlan>();
-    for (Part& p : split(nodes, seg, sc.cut_adds != 0, sc.layout == 1 ? 1 : 32)) {
+    for (Part& p : split(nodes, seg, sc.cut_adds != 0, sc.layout >= 1 ? 1 : 32)) {
       if (p.order.empty() && p.pops.empty()) continue;
       if (p.inputs.size() > kMaxInputs) throw RuntimeError("fused: too many inputs in one segment");
       np->kernels.push_back(part_kernel(nodes, p, N, sc, compile_ms));
@@ -1407,7 +1624,48 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
     int64_t range = 0;
     int blocks = 1;
     const int per_sm = sc.ctas_per_sm > 0 ? std::min(sc.ctas_per_sm, c.blocks_per_sm) : c.blocks_per_sm;
-    if (sc.layout == 1) {
+    std::vector<uint8_t> targs;   // the TMA form's argument block
+    if (pk.roww > 0) {
+      const int R = pk.roww;
+      const int per = sc.ctas_per_sm > 0 ? std::min(sc.ctas_per_sm, pk.tma_blocks_per_sm) : pk.tma_blocks_per_sm;
+      const int64_t threads_cap = static_cast<int64_t>(dev.sm_count()) * per * sc.warps * 32;
+      const int64_t min_range = std::max<int64_t>(64, 16 * pk.warm);
+      int64_t threads = std::max<int64_t>(1, std::min(threads_cap, (nw + min_range - 1) / min_range));
+      range = ((nw + threads - 1) / threads + R - 1) / R * R;
+      range = std::min<int64_t>(std::max<int64_t>(range, R), int64_t(1) << 25);
+      const int64_t total = (nw + range - 1) / range;
+      blocks = static_cast<int>((total + sc.warps * 32 - 1) / (sc.warps * 32));
+      const int64_t nfull = nw / range;
+      const int nm = static_cast<int>(pk.mapped.size());
+      const int nmp = std::max(1, nm), nop = std::max(1, static_cast<int>(p.outputs.size()));
+      const size_t maps_bytes = 128 * static_cast<size_t>(nmp + nop);
+      targs.assign(((maps_bytes + 8 * (ni + no + 6)) + 63) / 64 * 64, 0);
+      auto encode = [&](void* dst, const uint64_t* base) {
+        cuuint64_t dims[3] = {static_cast<cuuint64_t>(R), static_cast<cuuint64_t>(range / R),
+                              static_cast<cuuint64_t>(nfull)};
+        cuuint64_t strides[2] = {static_cast<cuuint64_t>(R) * 8, static_cast<cuuint64_t>(range) * 8};
+        cuuint32_t box[3] = {static_cast<cuuint32_t>(R), 1, 32};
+        cuuint32_t es[3] = {1, 1, 1};
+        BSZ_CU(drv().tensor_map_encode_tiled(
+            reinterpret_cast<CUtensorMap*>(dst), CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, const_cast<uint64_t*>(base), dims,
+            strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            R == 4 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE));
+      };
+      if (nfull > 0) {
+        for (int k = 0; k < nm; ++k) encode(targs.data() + 128 * k, reinterpret_cast<const uint64_t*>(args[pk.mapped[k]]));
+        for (size_t o = 0; o < p.outputs.size(); ++o)
+          encode(targs.data() + 128 * (nmp + o), reinterpret_cast<const uint64_t*>(args[ni + o]));
+      }
+      uint64_t* tail = reinterpret_cast<uint64_t*>(targs.data() + maps_bytes);
+      for (int i = 0; i < ni + no; ++i) tail[i] = args[i];
+      tail[ni + no + 0] = reinterpret_cast<uint64_t>(d_slots);
+      tail[ni + no + 1] = reinterpret_cast<uint64_t>(impl_->d_fail);
+      tail[ni + no + 2] = static_cast<uint64_t>(nw);
+      tail[ni + no + 3] = static_cast<uint64_t>(range);
+      tail[ni + no + 4] = mask_for_bits(N);
+      tail[ni + no + 5] = static_cast<uint64_t>(nfull);
+    } else if (sc.layout >= 1) {
       // thread-sequential: one range of whole 4-word chunks per thread, at
       // least 16 warm-ups long; a persistent grid of what stays resident
       const int64_t threads_cap = sc.ctas_per_sm < 0 ? std::numeric_limits<int64_t>::max() / 2
@@ -1438,10 +1696,10 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
     args[ni + no + 3] = static_cast<uint64_t>(range);
     args[ni + no + 4] = mask_for_bits(N);
     BSZ_CUDA(cudaMemsetAsync(impl_->d_fail, 0, 4, dev.stream()));
-    void* kparams[] = {args.data()};
+    void* kparams[] = {pk.roww > 0 ? static_cast<void*>(targs.data()) : static_cast<void*>(args.data())};
     {
       ProfScope prof(dev, "fused");
-      BSZ_CU(drv().launch_kernel(c.fn, blocks, 1, 1, sc.warps * 32, 1, 1, 0,
+      BSZ_CU(drv().launch_kernel(c.fn, blocks, 1, 1, sc.warps * 32, 1, 1, pk.roww > 0 ? pk.smem : 0,
                             reinterpret_cast<CUstream>(dev.stream()), kparams, nullptr));
     }
     ++dev.n_launches;

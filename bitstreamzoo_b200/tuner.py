@@ -50,18 +50,31 @@ from . import DEFAULT_SCHEDULE, MODE_FUSED, BszError
 # so the searched space leaves them out.
 CODEGEN_AXES = {"warps": (4, 8), "min_blocks": (2, 4), "prefetch": (0, 1), "cut_adds": (0,)}
 LAUNCH_AXES = {"ctas_per_sm": (0, 2)}
+# The thread-sequential form (layout 1): its register-resident chunk needs
+# the full register file (min_blocks 1; at min_blocks 2 the 2,000-op regex
+# DAG spills and runs 2x slower), and prefetch / range_steps do not apply.
+SEQ_AXES = {"layout": (1,), "warps": (4, 8), "min_blocks": (1,), "prefetch": (0,), "cut_adds": (0,),
+            "ctas_per_sm": (0,)}
 
 
-def candidate_space(codegen=None, launch=None) -> list[dict]:
-    """Cartesian product of the axes, each a full schedule dict."""
+def candidate_space(codegen=None, launch=None, seq=None) -> list[dict]:
+    """Cartesian product of the axes, each a full schedule dict: the warp
+    form's codegen x launch axes, then the thread-sequential form's axes
+    (``seq``; pass an empty dict to leave that form out)."""
     codegen = codegen or CODEGEN_AXES
     launch = launch or LAUNCH_AXES
+    seq = SEQ_AXES if seq is None else seq
     keys = list(codegen) + list(launch)
     out = []
     for vals in itertools.product(*[codegen[k] for k in codegen], *[launch[k] for k in launch]):
         s = dict(DEFAULT_SCHEDULE)
         s.update(dict(zip(keys, vals)))
         out.append(s)
+    if seq:
+        for vals in itertools.product(*[seq[k] for k in seq]):
+            s = dict(DEFAULT_SCHEDULE)
+            s.update(dict(zip(list(seq), vals)))
+            out.append(s)
     return out
 
 

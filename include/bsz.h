@@ -76,7 +76,10 @@ typedef struct bsz_schedule {
   int32_t cut_adds;     /* 1: materialize every addition (one kernel per addition level) */
   int32_t layout;       /* 0: each warp walks a word range, lane = word (cross-word state by
                            ballots and shuffles); 1: each thread walks its own word range
-                           (cross-word state in registers, 256-bit per-thread accesses) */
+                           (cross-word state in registers, 256-bit per-thread accesses);
+                           2: as 1, with every input and output moved by TMA boxes of
+                           chunk_words words x 32 threads through shared memory */
+  int32_t chunk_words;  /* layout 2: 4 or 8 words per thread per box */
 } bsz_schedule;
 
 /* ---- library ---------------------------------------------------------- */

@@ -20,8 +20,12 @@ from oracle import cwords, pyoracle
 import progen
 
 
-# fused forms: warp ranges with lane = word, and thread-sequential ranges
-FORMS = [(bz.MODE_PLAIN, None), (bz.MODE_FUSED, {"layout": 0}), (bz.MODE_FUSED, {"layout": 1})]
+# fused forms: warp ranges with lane = word, thread-sequential ranges with
+# register chunks, and thread-sequential ranges through TMA boxes (8- and
+# 4-word rows; streams under 2^16 words take the register form instead)
+FORMS = [(bz.MODE_PLAIN, None), (bz.MODE_FUSED, {"layout": 0}), (bz.MODE_FUSED, {"layout": 1}),
+         (bz.MODE_FUSED, {"layout": 2, "warps": 4, "min_blocks": 1}),
+         (bz.MODE_FUSED, {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1})]
 
 
 def run_both(ctx, src, nbits, inputs):
@@ -39,7 +43,7 @@ def run_both(ctx, src, nbits, inputs):
                 raise AssertionError(f"mode {mode} {sched} output {name}: first bad word {bad} of {got.size}")
         for name, v in ref_pops.items():
             assert r.int(name) == v, (mode, sched, name)
-        results[(mode, (sched or {}).get("layout"))] = r.stats
+        results[(mode, (sched or {}).get("layout"), (sched or {}).get("chunk_words"))] = r.stats
     return results
 
 
@@ -53,8 +57,9 @@ def bz_mask(nbits):
 def test_long_streams(ctx, nbits):
     inputs = wl.long_streams_inputs(nbits, seed=nbits)
     st = run_both(ctx, wl.long_streams_src(), nbits, inputs)
-    assert st[(bz.MODE_FUSED, 0)]["n_fused_launches"] >= 1
-    assert st[(bz.MODE_FUSED, 1)]["n_fused_launches"] >= 1
+    for key, v in st.items():
+        if key[0] == bz.MODE_FUSED:
+            assert v["n_fused_launches"] >= 1, key
 
 
 @pytest.mark.gpu
@@ -65,9 +70,10 @@ def test_matchstar(ctx):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n_ops,seed", [(300, 1), (300, 2), (2000, 3)])
-def test_regex_dag(ctx, n_ops, seed):
-    nbits = (1 << 20) + 64 * 3 + 11
+@pytest.mark.parametrize("n_ops,seed,nbits", [(300, 1, (1 << 20) + 64 * 3 + 11), (300, 2, (1 << 20) + 64 * 3 + 11),
+                                              (2000, 3, (1 << 20) + 64 * 3 + 11), (2000, 4, (1 << 23) + 5),
+                                              (2000, 5, 1 << 24)])
+def test_regex_dag(ctx, n_ops, seed, nbits):
     src = wl.regex_dag_src(n_ops=n_ops, seed=seed)
     inputs = wl.regex_dag_inputs(nbits, seed=seed)
     run_both(ctx, src, nbits, inputs)
@@ -94,8 +100,9 @@ def test_unresolvable_carry_falls_back_exactly(ctx):
     rng = np.random.default_rng(4)
     inputs = {"x": wl.random_words(rng, nbits), "z": wl.random_words(rng, nbits)}
     st = run_both(ctx, src, nbits, inputs)
-    assert st[(bz.MODE_FUSED, 0)]["n_fused_fallbacks"] >= 1
-    assert st[(bz.MODE_FUSED, 1)]["n_fused_fallbacks"] >= 1
+    for key, v in st.items():
+        if key[0] == bz.MODE_FUSED:
+            assert v["n_fused_fallbacks"] >= 1, key
 
 
 @pytest.mark.gpu

@@ -19,7 +19,12 @@ def test_candidate_space_is_the_product():
     for ax in (tuner.CODEGEN_AXES, tuner.LAUNCH_AXES):
         for v in ax.values():
             n *= len(v)
+    m = 1
+    for v in tuner.SEQ_AXES.values():
+        m *= len(v)
+    n += m
     assert len(c) == n == len(tuner.CANDIDATES)
+    assert sum(1 for s in c if s["layout"] == 1) == m
     assert len({tuner.schedule_key(s) for s in c}) == n
     for s in c:
         assert set(s) == set(DEFAULT_SCHEDULE)
