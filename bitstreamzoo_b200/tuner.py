@@ -86,16 +86,20 @@ def schedule_key(s: dict) -> tuple:
 
 
 def encode_schedule(s: dict) -> list[float]:
-    """Schedule features (7): log2 warps, log2 min_blocks, occupancy cap
+    """Schedule features (10): log2 warps, log2 min_blocks, occupancy cap
     (0 = none), log2 range_steps, prefetch, cut_adds, log2 threads x
-    min_blocks (the register cap's denominator)."""
+    min_blocks (the register cap's denominator), thread-sequential form,
+    TMA form, log2 chunk words (TMA form; 0 otherwise)."""
+    layout = int(s.get("layout", 0))
     return [math.log2(s["warps"]), math.log2(max(1, s["min_blocks"])),
-            math.log2(1 + s["ctas_per_sm"]), math.log2(max(1, s["range_steps"])),
+            math.log2(1 + max(0, s["ctas_per_sm"])), math.log2(max(1, s["range_steps"])),
             float(s["prefetch"]), float(s["cut_adds"]),
-            math.log2(32 * s["warps"] * max(1, s["min_blocks"]))]
+            math.log2(32 * s["warps"] * max(1, s["min_blocks"])),
+            float(layout >= 1), float(layout == 2),
+            math.log2(s.get("chunk_words", 8)) if layout == 2 else 0.0]
 
 
-N_SCHEDULE_FEATURES = 7
+N_SCHEDULE_FEATURES = 10
 N_PROGRAM_FEATURES = 15
 N_FEATURES = N_PROGRAM_FEATURES + 1 + N_SCHEDULE_FEATURES + 1
 
@@ -119,7 +123,8 @@ def register_pressure(pfeat: list[float], sched: dict) -> float:
     plus ~16 of bookkeeping) over the register cap the schedule's launch
     bounds allow: above 0 the generated kernel spills."""
     peak = 2 ** pfeat[14] - 1
-    cap = min(255.0, 65536.0 / (32 * sched["warps"] * max(1, sched["min_blocks"])))
+    blocks = 1 if int(sched.get("layout", 0)) == 2 else max(1, sched["min_blocks"])
+    cap = min(255.0, 65536.0 / (32 * sched["warps"] * blocks))
     return math.log2(2 * peak + 16) - math.log2(cap)
 
 
@@ -388,13 +393,72 @@ def _device_inputs(nbits: int, n_inputs: int, seed: int):
     return bufs, {f"b{i}": (b.data_ptr(), nw) for i, b in enumerate(bufs)}
 
 
+CODEGEN_KEYS = ("warps", "min_blocks", "prefetch", "cut_adds", "layout", "chunk_words")
+
+
 def codegen_key(s: dict) -> tuple:
-    return tuple(int(s[k]) for k in CODEGEN_AXES)
+    """The knobs that change the generated source (one NVRTC compile each)."""
+    return tuple(int(s.get(k, DEFAULT_SCHEDULE[k])) for k in CODEGEN_KEYS)
 
 
-def study(ctx, train_srcs, test_srcs, sizes=(1 << 23, 1 << 25, 1 << 27), candidates=None,
+def precompile(srcs, candidates=None, nbits: int = 1 << 22, threads: int | None = None, log=None) -> float:
+    """Compiles the fused kernels of every (program, code variant) pair
+    ahead of timing, in parallel host threads, each with its own context
+    (NVRTC runs on the host; the process-wide kernel cache then serves the
+    timing runs).  Kernels do not depend on the stream length beyond its
+    word alignment, so one short run per pair (``nbits``, a multiple of 64
+    long enough for every form) compiles what every length uses.  Returns
+    the wall seconds."""
+    import concurrent.futures as cf
+    import threading
+    import time as _time
+
+    from . import Context
+
+    candidates = candidates or CANDIDATES
+    reps = {}
+    for s in candidates:
+        reps.setdefault(codegen_key(s), s)
+    jobs = [(src, s) for src in srcs for s in reps.values()]
+    local = threading.local()
+    ctxs = []
+    lock = threading.Lock()
+    nw = (nbits + 63) // 64
+    rng = np.random.default_rng(7)
+    host_in = [rng.integers(0, 2**64, size=nw, dtype=np.uint64) for _ in range(8)]
+
+    def work(job):
+        if not hasattr(local, "ctx"):
+            local.ctx = Context(0)
+            local.progs = {}
+            with lock:
+                ctxs.append(local.ctx)
+        src, sched = job
+        prog = local.progs.get(src)
+        if prog is None:
+            prog = local.progs[src] = local.ctx.compile(src)
+        r = prog.run(nbits, MODE_FUSED)
+        r.set_schedule(sched)
+        for i in range(8):
+            try:
+                r.bind(f"b{i}", host_in[i])
+            except BszError:
+                pass   # the program has fewer inputs
+        r.execute()
+
+    t0 = _time.time()
+    with cf.ThreadPoolExecutor(max_workers=threads or min(16, os.cpu_count() or 4)) as ex:
+        for k, _ in enumerate(ex.map(work, jobs)):
+            if log and (k + 1) % 200 == 0:
+                log(f"precompiled {k + 1}/{len(jobs)} t={_time.time() - t0:.0f}s")
+    for c in ctxs:
+        c.close()
+    return _time.time() - t0
+
+
+def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candidates=None,
           sample_frac: float = 0.5, reps: int = 3, steps: int = 1500, seed: int = 0, log=None,
-          weight_decay: float = 0.05) -> dict:
+          weight_decay: float = 0.05, precompile_threads: int = 0) -> dict:
     """Collects timings, fits a :class:`CostModel` and reports pick regret on
     the held-out programs for the model's top-1 and top-4 picks and for the
     default schedule.
@@ -422,10 +486,18 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 23, 1 << 25, 1 << 27), candida
 
     groups = []
     variants = sorted({codegen_key(s) for s in candidates})
+    chosen_by = []
+    for i in range(len(train_srcs)):
+        k = max(1, int(round(sample_frac * len(variants))))
+        chosen_by.append({variants[j] for j in rng.choice(len(variants), size=k, replace=False)})
+    if precompile_threads:
+        t_pc = precompile(train_srcs + test_srcs, candidates, threads=precompile_threads, log=log)
+        if log:
+            log(f"precompiled in {t_pc:.0f}s")
+    t0 = _time.time()
     for i, src in enumerate(train_srcs):
         prog, pf = prog_of(src)
-        k = max(1, int(round(sample_frac * len(variants))))
-        chosen = {variants[j] for j in rng.choice(len(variants), size=k, replace=False)}
+        chosen = chosen_by[i]
         for n in sizes:
             for s in candidates:
                 if codegen_key(s) not in chosen:
@@ -460,11 +532,16 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 23, 1 << 25, 1 << 27), candida
             ranked = model.rank(pf, n, candidates)
             top4 = min(times[schedule_key(s)] for s in ranked[:4])
             best = min(times.values())
+            cand_ms = [times[schedule_key(s)] for s in candidates]
             rows.append({"program": i, "ops": int(round(2 ** pf[0] - 1)), "bits": n, "best_ms": best,
                          "best": list(min(times, key=times.get)),
                          "regret_top1": times[schedule_key(ranked[0])] / best - 1,
                          "regret_top4": top4 / best - 1,
-                         "regret_default": times[default_key] / best - 1})
+                         "regret_default": times[default_key] / best - 1,
+                         # a uniformly random pick from the space, in expectation
+                         "regret_random": float(np.mean(cand_ms)) / best - 1,
+                         "tuning_ms_exhaustive": float(sum(cand_ms)) * (reps + 1),
+                         "tuning_ms_top4": float(sum(times[schedule_key(s)] for s in ranked[:4])) * (reps + 1)})
         if log:
             log(f"test {i + 1}/{len(test_srcs)} t={_time.time() - t0:.0f}s")
 
@@ -477,7 +554,10 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 23, 1 << 25, 1 << 27), candida
             "n_train_timings": n_timed, "loss_first": float(np.mean(losses[:20])),
             "loss_last": float(np.mean(losses[-20:])), "collect_s": t_collect, "fit_s": t_fit,
             "regret_top1": stats("regret_top1"), "regret_top4": stats("regret_top4"),
-            "regret_default": stats("regret_default"),
+            "regret_default": stats("regret_default"), "regret_random": stats("regret_random"),
+            "top1_beats_default_frac": float(np.mean([r["regret_top1"] <= r["regret_default"] for r in rows])),
+            "device_time_saved_top4": 1.0 - float(np.sum([r["tuning_ms_top4"] for r in rows]) /
+                                                  np.sum([r["tuning_ms_exhaustive"] for r in rows])),
             "exhaustive_timings_per_case": len(candidates),
             # every timing, for offline study of the model
             "raw": {"train_X": X, "train_ms": y, "train_groups": groups, "test": raw_test}}
@@ -497,11 +577,13 @@ def main(argv=None):
     ap.add_argument("--test", type=int, default=8)
     ap.add_argument("--sample-frac", type=float, default=0.5)
     ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--max-ops", type=int, default=3000)
+    ap.add_argument("--threads", type=int, default=16, help="parallel precompile threads (0: none)")
     a = ap.parse_args(argv)
     ctx = Context(0)
-    train, test = tuning_suite(a.train, a.test)
+    train, test = tuning_suite(a.train, a.test, max_ops=a.max_ops)
     rep = study(ctx, train, test, sample_frac=a.sample_frac, steps=a.steps,
-                log=lambda m: print(m, flush=True))
+                log=lambda m: print(m, flush=True), precompile_threads=a.threads)
     model = rep.pop("model")
     if a.out:
         model.save(a.out)
