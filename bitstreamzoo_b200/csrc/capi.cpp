@@ -555,6 +555,8 @@ bsz_batch* bsz_batch_create(bsz_ctx* ctx, bsz_program* const* programs, int n_pr
           s.min_blocks = std::max(1, schedule->min_blocks);
           s.prefetch = schedule->prefetch;
           s.cut_adds = 0;
+          s.layout = std::max(0, std::min(schedule->layout, 2));
+          s.chunk_words = schedule->chunk_words == 4 ? 4 : 8;
         }
         b->runner = std::make_unique<bsz::BatchRunner>(*ctx->dev, progs, std::move(inst), s);
         for (auto* p : b->progs) ++p->refs;

@@ -697,12 +697,25 @@ struct GenSeq {
   int roww = 8;
   int stages = 2;
   std::vector<int> mapped;           // input indices (A.in order) that are read through boxes
+  // batches: fixed argument positions and outputs that may be skipped (null)
+  bool guard_outputs = false;
+  const std::map<int, int>* in_index_override = nullptr;
+  const std::vector<std::pair<int, int>>* outs_override = nullptr;
 
   std::string v(int n) const { return "v" + std::to_string(n); }
 
   void analyze() {
-    for (size_t i = 0; i < part.inputs.size(); ++i) in_idx[part.inputs[i]] = static_cast<int>(i);
-    for (size_t i = 0; i < part.outputs.size(); ++i) outs.push_back({part.outputs[i], static_cast<int>(i)});
+    if (in_index_override) {
+      for (int n : part.inputs) {
+        auto it = in_index_override->find(n);
+        in_idx[n] = it == in_index_override->end() ? 0 : it->second;   // constants: index unused
+      }
+    } else {
+      for (size_t i = 0; i < part.inputs.size(); ++i) in_idx[part.inputs[i]] = static_cast<int>(i);
+    }
+    if (outs_override) outs = *outs_override;
+    else
+      for (size_t i = 0; i < part.outputs.size(); ++i) outs.push_back({part.outputs[i], static_cast<int>(i)});
     for (int n : part.order) in_part.insert(n);
     dyn.assign(nodes.size(), 0);
     int64_t max_static = 0;
@@ -916,8 +929,11 @@ struct GenSeq {
     return std::to_string(it == sdh.end() ? 0 : it->second);
   }
 
+  std::string guard(int o) const {
+    return guard_outputs ? "if (A.out[" + std::to_string(o) + "]) " : std::string();
+  }
   void emit_store_word(std::ostringstream& s) const {
-    for (auto& kv : outs) s << "      A.out[" << kv.second << "][w] = " << v(kv.first) << ";\n";
+    for (auto& kv : outs) s << "      " << guard(kv.second) << "A.out[" << kv.second << "][w] = " << v(kv.first) << ";\n";
     for (size_t j = 0; j < part.pops.size(); ++j) s << "      pc" << j << " += __popcll(" << v(part.pops[j].first) << ");\n";
   }
 
@@ -1075,7 +1091,14 @@ struct GenSeq {
     compute_mapped();
     std::ostringstream s;
     const int ni = static_cast<int>(part.inputs.size()), no = static_cast<int>(part.outputs.size());
-    s << Gen::args_struct(ni, no);
+    s << Gen::args_struct(ni, no) << helpers();
+    emit_kernel(s, ni, no);
+    return s.str();
+  }
+
+  // Device helpers shared by every thread-sequential kernel / device function.
+  static std::string helpers() {
+    std::ostringstream s;
     s << "template <int K> __device__ __forceinline__ u64 fshl(u64 x, u64 p) {\n"
          "  const u32 xl = (u32)x, xh = (u32)(x >> 32), pl = (u32)p, ph = (u32)(p >> 32);\n"
          "  u32 lo, hi;\n"
@@ -1101,7 +1124,21 @@ struct GenSeq {
          "  asm volatile(\"ld.global.nc.L2::128B.v4.u64 {%0,%1,%2,%3}, [%4];\" : \"=l\"(a), \"=l\"(b), \"=l\"(c), \"=l\"(d) : \"l\"(p));\n}\n"
          "__device__ __forceinline__ void st4(u64* p, u64 a, u64 b, u64 c, u64 d) {\n"
          "  asm volatile(\"st.global.v4.u64 [%0], {%1,%2,%3,%4};\" :: \"l\"(p), \"l\"(a), \"l\"(b), \"l\"(c), \"l\"(d) : \"memory\");\n}\n";
-    if (tma) {
+    return s.str();
+  }
+
+  // The kernel (or, with `fn_name`, the batch device function for one work
+  // item [s_item, e_item) of one instance, split into 32 lane ranges).
+  void emit_kernel(std::ostringstream& s, int ni, int no, const std::string& fn_name = "") const {
+    if (!fn_name.empty()) {
+      s << "__device__ __noinline__ void " << fn_name
+        << "(const Args* __restrict__ Ap, const long long s_item, const long long e_item, const int lane) {\n"
+        << "  const Args& A = *Ap;\n"
+        << "  const long long L = (((e_item - s_item) + 31) / 32 + 3) / 4 * 4;\n"
+        << "  const long long s = s_item + lane * L;\n"
+        << "  const bool active = s < e_item;\n"
+        << "  const long long e = min(s + L, e_item);\n";
+    } else if (tma) {
       s << tma_prelude(ni, no);
       s << "extern \"C\" __global__ void __launch_bounds__(" << warps * 32 << ", 1)\n"
         << "bsz_fused(const __grid_constant__ ArgsT A) {\n";
@@ -1109,11 +1146,12 @@ struct GenSeq {
       s << "extern \"C\" __global__ void __launch_bounds__(" << warps * 32 << ", " << min_blocks
         << ")\nbsz_fused(const Args A) {\n";
     }
-    s << "  const int lane = threadIdx.x & 31;\n"
-      << "  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
-      << "  const long long s = tid * A.range;\n"
-      << "  const bool active = s < A.nw;\n"
-      << "  const long long e = min(s + A.range, A.nw);\n";
+    if (fn_name.empty())
+      s << "  const int lane = threadIdx.x & 31;\n"
+        << "  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
+        << "  const long long s = tid * A.range;\n"
+        << "  const bool active = s < A.nw;\n"
+        << "  const long long e = min(s + A.range, A.nw);\n";
     std::vector<int> adds;
     for (int n : part.order)
       if (nodes[n].op == NOp::Add) adds.push_back(n);
@@ -1191,7 +1229,8 @@ struct GenSeq {
     }
     for (auto& kv : outs) {
       const std::string o = std::to_string(kv.second);
-      s << "      st4(A.out[" << o << "] + c, r" << o << "_0, r" << o << "_1, r" << o << "_2, r" << o << "_3);\n";
+      s << "      " << guard(kv.second) << "st4(A.out[" << o << "] + c, r" << o << "_0, r" << o << "_1, r" << o << "_2, r" << o
+        << "_3);\n";
     }
     s << "      w += 4;\n    } else {\n      {\n";
     emit_word(s, 's', 0);
@@ -1205,6 +1244,13 @@ struct GenSeq {
         << "    if (lane == 0 && t) atomicAdd(A.slots + " << part.pops[j].second << ", t);\n  }\n";
     }
     s << "}\n";
+  }
+
+  // Batch device function (register chunks; see emit_kernel).
+  std::string device_function(const std::string& name) {
+    analyze();
+    std::ostringstream s;
+    emit_kernel(s, 0, 0, name);
     return s.str();
   }
 };
@@ -1890,24 +1936,53 @@ BatchRunner::BatchRunner(Device& dev, const std::vector<const Program*>& progs,
   m.sched = sched;
   m.srcs = progs;
   m.inst = std::move(instances);
+  // the thread-sequential form (register chunks; batches have no TMA form)
+  // needs every instance buffer 32-byte aligned
+  bool seq = sched.layout >= 1;
+  for (const BatchInstance& bi : m.inst) {
+    for (const uint64_t* q : bi.inputs)
+      if (reinterpret_cast<uintptr_t>(q) & 31) seq = false;
+    for (const uint64_t* q : bi.outputs)
+      if (reinterpret_cast<uintptr_t>(q) & 31) seq = false;
+  }
   // 1. trace every program symbolically and plan its DAG
   ExecOptions eo;
   eo.mode = ExecMode::Fused;
   eo.sched = sched;
   std::string fns;
+  std::vector<BatchProg> traced(progs.size());
   for (size_t k = 0; k < progs.size(); ++k) {
-    BatchProg bp;
     {
       Executor ex(dev, *progs[k], int64_t(1) << 20, eo);
-      bp.t = ex.trace();
+      traced[k].t = ex.trace();
     }
-    plan_batch_program(bp);
-    Gen g{bp.t.nodes, bp.part, 0, sched.warps, sched.min_blocks, true, sched.prefetch != 0};
-    g.guard_outputs = true;
-    g.in_index_override = &bp.in_index;
-    g.outs_override = &bp.outs;
-    bp.fn = g.device_function("dag_" + std::to_string(k));
-    bp.warm = g.warm;
+    plan_batch_program(traced[k]);
+    // a temporary shifted left by 64 bits or more needs words a lane no
+    // longer holds: such programs keep the warp form
+    for (int n : traced[k].part.order) {
+      const Node& x = traced[k].t.nodes[n];
+      const NOp ao = x.a >= 0 ? traced[k].t.nodes[x.a].op : NOp::Buf;
+      const bool temp = ao != NOp::Buf && ao != NOp::Zero && ao != NOp::OnesMask && ao != NOp::AllOnes;
+      if (x.op == NOp::Shl && temp && x.k >= 64) seq = false;
+    }
+  }
+  for (size_t k = 0; k < progs.size(); ++k) {
+    BatchProg bp = std::move(traced[k]);
+    if (seq) {
+      GenSeq g{bp.t.nodes, bp.part, 0, sched.warps, sched.min_blocks, true};
+      g.guard_outputs = true;
+      g.in_index_override = &bp.in_index;
+      g.outs_override = &bp.outs;
+      bp.fn = g.device_function("dag_" + std::to_string(k));
+      bp.warm = g.warm;
+    } else {
+      Gen g{bp.t.nodes, bp.part, 0, sched.warps, sched.min_blocks, true, sched.prefetch != 0};
+      g.guard_outputs = true;
+      g.in_index_override = &bp.in_index;
+      g.outs_override = &bp.outs;
+      bp.fn = g.device_function("dag_" + std::to_string(k));
+      bp.warm = g.warm;
+    }
     m.max_in = std::max<int>(m.max_in, static_cast<int>(bp.t.input_nodes.size()));
     m.max_out = std::max<int>(m.max_out, static_cast<int>(bp.t.output_nodes.size()));
     fns += bp.fn;
@@ -1915,7 +1990,7 @@ BatchRunner::BatchRunner(Device& dev, const std::vector<const Program*>& progs,
   }
   // 2. one kernel: every program's DAG as a device function + a work loop
   std::ostringstream src;
-  src << Gen::args_struct(m.max_in, m.max_out) << fns
+  src << Gen::args_struct(m.max_in, m.max_out) << (seq ? GenSeq::helpers() : std::string()) << fns
       << "struct Item { int inst; int dag; long long s; long long e; };\n"
       << "extern \"C\" __global__ void __launch_bounds__(" << sched.warps * 32 << ", "
       << sched.min_blocks << ")\nbsz_batch(const Args* __restrict__ insts, "
@@ -1949,7 +2024,10 @@ BatchRunner::BatchRunner(Device& dev, const std::vector<const Program*>& progs,
     m.slot_base.push_back(m.n_slots);
     m.n_slots += static_cast<int64_t>(bp.t.pops.size());
     const int64_t nw = std::max<int64_t>(1, (bi.bitlength + 63) / 64);
-    const int64_t range = 32 * std::max<int64_t>(sched.range_steps, (bp.warm / 32) * 8);
+    // work items: warp form, runs of 32-word steps; thread-sequential form,
+    // 32 lane ranges of whole 4-word chunks, each at least 16 warm-ups long
+    const int64_t range = seq ? 128 * ((std::max<int64_t>(64, 16 * bp.warm) + 3) / 4)
+                              : 32 * std::max<int64_t>(sched.range_steps, (bp.warm / 32) * 8);
     for (int64_t s0 = 0; s0 < nw; s0 += range)
       items.push_back({static_cast<int32_t>(i), bi.program, s0, std::min(nw, s0 + range)});
     uint64_t* a = args.data() + stride * i;

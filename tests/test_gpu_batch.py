@@ -65,7 +65,9 @@ def test_batched_mixed_programs_and_ragged_lengths(ctx):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("schedule", [{"warps": 2, "range_steps": 32, "prefetch": 0},
-                                      {"warps": 8, "range_steps": 256, "min_blocks": 2}])
+                                      {"warps": 8, "range_steps": 256, "min_blocks": 2},
+                                      {"layout": 1, "warps": 4, "min_blocks": 1},
+                                      {"layout": 1, "warps": 8, "min_blocks": 1}])
 def test_batched_schedules(ctx, schedule):
     srcs, plan = wl.batched_plan(n_instances=40, n_dags=4, lo_log2=12, hi_log2=20, ops=200, seed=9)
     _run_batch(ctx, srcs, plan, seed=3, schedule=schedule)
@@ -78,3 +80,15 @@ def test_batch_rejects_programs_with_control_flow(ctx):
     t = torch.zeros(4, dtype=torch.int64, device="cuda")
     with pytest.raises(bz.BszError):
         bz.Batch(ctx, [p], [(0, 200, [t.data_ptr()], [t.data_ptr()])])
+
+
+@pytest.mark.gpu
+def test_batched_thread_sequential_uneven_and_ragged(ctx):
+    """The thread-sequential batch form on uneven regex DAG instances and on
+    ragged lengths (instances shorter than one lane chunk, masked last words)."""
+    srcs, plan = wl.batched_plan(n_instances=64, n_dags=8, lo_log2=6, hi_log2=21, ops=300, seed=15)
+    _run_batch(ctx, srcs, plan, seed=4, schedule={"layout": 1, "warps": 4, "min_blocks": 1})
+    srcs = [wl.long_streams_src(), wl.MATCHSTAR_SRC, wl.regex_dag_src(300, seed=11)]
+    plan = [(k % 3, bits) for k, bits in enumerate([1, 63, 64, 65, 4095, 4096, 100003, 1 << 20,
+                                                     (1 << 21) + 7, 777, 2 ** 17 + 1, 5])]
+    _run_batch(ctx, srcs, plan, seed=6, schedule={"layout": 1, "warps": 8, "min_blocks": 1})
