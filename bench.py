@@ -589,7 +589,10 @@ def measure_workload(E, workload: str, nbits: int, steps: int, warmup: int, main
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tpath):
             with open(tpath) as f:
-                traffic = json.load(f).get(f"{workload}:{kname}:layout{sched.get('layout', 0)}")
+                tj = json.load(f)
+            # per kernel form: the fused kernel's traffic depends on the layout
+            traffic = tj.get(f"{workload}:{kname}:layout{sched.get('layout', 0)}") if kname.startswith("fused") \
+                else tj.get(f"{workload}:{kname}")
         roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": E.hbm,
                 "peak_source": E.hbm_src, "unit": "GB/s", "frac": achieved / E.hbm,
                 "traffic": traffic, "bytes_per_launch": bytes_launch,
