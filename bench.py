@@ -696,9 +696,30 @@ def measure_batched(E, instances: int, steps: int, warmup: int):
         in_bytes += 8 * bits // 8
         out_bytes += 4 * bits // 8 + 4 * 8
     torch.cuda.synchronize()
-    t0 = time.time()
-    b = bz.Batch(ctx, progs, insts)
-    build_s = time.time() - t0
+    # schedule: the warp form and the thread-sequential form, each timed over
+    # 3 launches before the timed region; the faster one is measured
+    cands = [dict(bz.DEFAULT_SCHEDULE), dict(bz.DEFAULT_SCHEDULE, layout=1, warps=8, min_blocks=1)]
+    tried = []
+    build_s = 0.0
+    for sc in cands:
+        t0 = time.time()
+        bb = bz.Batch(ctx, progs, insts, sc)
+        build_s += time.time() - t0
+        bb.launch()
+        bb.finish()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(E.ext)
+        for _ in range(3):
+            bb.launch()
+        e1.record(E.ext)
+        bb.finish()
+        e1.synchronize()
+        tried.append((e0.elapsed_time(e1) / 3, sc))
+        del bb
+    tried.sort(key=lambda x: x[0])
+    sched = tried[0][1]
+    b = bz.Batch(ctx, progs, insts, sched)
     for _ in range(max(3, warmup)):
         b.launch()
         b.finish()
@@ -747,7 +768,9 @@ def measure_batched(E, instances: int, steps: int, warmup: int):
                                "lengths log-uniform in [2^12, 2^26] bits, 8 inputs / 4 outputs + 4 popcounts each",
                    "input_bytes": in_bytes, "output_bytes": out_bytes, "work_items": b.items,
                    "build_s": build_s, "l2": "inputs (all instances) far larger than L2",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}", "schedule": sched,
+                   "schedule_source": "faster of the warp and thread-sequential forms over 3 launches each: "
+                                      + ", ".join(f"layout {sc.get('layout', 0)} {ms:.2f} ms" for ms, sc in tried)},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": E.hbm,
                      "peak_source": E.hbm_src, "unit": "GB/s", "frac": achieved / E.hbm, "traffic": None,
                      "bytes_per_launch": in_bytes + out_bytes, "launch_ms": launch_ms},

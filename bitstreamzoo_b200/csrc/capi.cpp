@@ -219,6 +219,7 @@ int bsz_run_set_schedule(bsz_run* run, const bsz_schedule* s) {
     c.cut_adds = s->cut_adds;
     c.layout = s->layout;
     c.chunk_words = s->chunk_words;
+    c.stages = s->stages;
     executor(run).set_schedule(c);
   });
 }
@@ -557,6 +558,7 @@ bsz_batch* bsz_batch_create(bsz_ctx* ctx, bsz_program* const* programs, int n_pr
           s.cut_adds = 0;
           s.layout = std::max(0, std::min(schedule->layout, 2));
           s.chunk_words = schedule->chunk_words == 4 ? 4 : 8;
+          s.stages = schedule->stages == 3 ? 3 : 2;
         }
         b->runner = std::make_unique<bsz::BatchRunner>(*ctx->dev, progs, std::move(inst), s);
         for (auto* p : b->progs) ++p->refs;

@@ -64,6 +64,7 @@ struct Schedule {
   int layout = 0;         // 0: warp ranges, lane = word; 1: thread-sequential ranges
                           // (register chunks); 2: thread-sequential ranges through TMA boxes
   int chunk_words = 8;    // layout 2: words per thread per box (4 or 8)
+  int stages = 2;         // layout 2: shared-memory stages of input boxes (2 or 3)
 };
 
 struct ExecOptions {

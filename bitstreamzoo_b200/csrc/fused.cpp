@@ -143,6 +143,7 @@ void FusedBackend::set_schedule(const Schedule& s) {
   c.min_blocks = std::max(1, std::min(c.min_blocks, 32));
   c.layout = std::max(0, std::min(c.layout, 2));
   c.chunk_words = c.chunk_words == 4 ? 4 : 8;
+  c.stages = c.stages == 3 ? 3 : 2;
   impl_->opt.sched = c;
 }
 
@@ -1510,6 +1511,7 @@ std::string graph_key(const std::vector<Node>& nodes, const std::vector<int>& or
   put(sc.cut_adds);
   put(sc.layout);
   put(sc.chunk_words);
+  put(sc.stages);
   return k;
 }
 
@@ -1555,6 +1557,7 @@ PartKernel part_kernel(const std::vector<Node>& nodes, const Part& p, int64_t N,
     GenSeq g{nodes, p, N, sc.warps, 1, (N % 64) != 0};
     g.tma = true;
     g.roww = sc.chunk_words == 4 ? 4 : 8;
+    g.stages = sc.stages == 3 ? 3 : 2;
     const std::string src = g.source();
     pk.c = compile_source(src, sc.warps * 32, compile_ms);
     pk.warm = g.warm;
@@ -1600,6 +1603,7 @@ bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& s
       GenSeq g{nodes, p, N, sc.warps, 1, (N % 64) != 0};
       g.tma = true;
       g.roww = sc.chunk_words == 4 ? 4 : 8;
+      g.stages = sc.stages == 3 ? 3 : 2;
       if (!is_compiled(g.source())) return false;
     } else if (sc.layout == 1) {
       GenSeq g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0};

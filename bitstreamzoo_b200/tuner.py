@@ -55,6 +55,12 @@ LAUNCH_AXES = {"ctas_per_sm": (0, 2)}
 # DAG spills and runs 2x slower), and prefetch / range_steps do not apply.
 SEQ_AXES = {"layout": (1,), "warps": (4, 8), "min_blocks": (1,), "prefetch": (0,), "cut_adds": (0,),
             "ctas_per_sm": (0,)}
+# The TMA form (layout 2): 4-word rows for 8 warps per CTA (2 or 3 stages),
+# 4-word rows for 4 warps (two CTAs per SM); 8-word rows leave room for only
+# 4 warps per SM and measured 1.7x slower on the regex DAG, so they are out.
+TMA_CANDIDATES = [{"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1, "prefetch": 0, "stages": 2},
+                  {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1, "prefetch": 0, "stages": 3},
+                  {"layout": 2, "chunk_words": 4, "warps": 4, "min_blocks": 1, "prefetch": 0, "stages": 2}]
 
 
 def candidate_space(codegen=None, launch=None, seq=None) -> list[dict]:
@@ -75,6 +81,10 @@ def candidate_space(codegen=None, launch=None, seq=None) -> list[dict]:
             s = dict(DEFAULT_SCHEDULE)
             s.update(dict(zip(list(seq), vals)))
             out.append(s)
+        for t in TMA_CANDIDATES:
+            s = dict(DEFAULT_SCHEDULE)
+            s.update(t)
+            out.append(s)
     return out
 
 
@@ -86,20 +96,21 @@ def schedule_key(s: dict) -> tuple:
 
 
 def encode_schedule(s: dict) -> list[float]:
-    """Schedule features (10): log2 warps, log2 min_blocks, occupancy cap
+    """Schedule features (11): log2 warps, log2 min_blocks, occupancy cap
     (0 = none), log2 range_steps, prefetch, cut_adds, log2 threads x
     min_blocks (the register cap's denominator), thread-sequential form,
-    TMA form, log2 chunk words (TMA form; 0 otherwise)."""
+    TMA form, log2 chunk words and stages (TMA form; 0 otherwise)."""
     layout = int(s.get("layout", 0))
     return [math.log2(s["warps"]), math.log2(max(1, s["min_blocks"])),
             math.log2(1 + max(0, s["ctas_per_sm"])), math.log2(max(1, s["range_steps"])),
             float(s["prefetch"]), float(s["cut_adds"]),
             math.log2(32 * s["warps"] * max(1, s["min_blocks"])),
             float(layout >= 1), float(layout == 2),
-            math.log2(s.get("chunk_words", 8)) if layout == 2 else 0.0]
+            math.log2(s.get("chunk_words", 8)) if layout == 2 else 0.0,
+            float(s.get("stages", 2)) if layout == 2 else 0.0]
 
 
-N_SCHEDULE_FEATURES = 10
+N_SCHEDULE_FEATURES = 11
 N_PROGRAM_FEATURES = 15
 N_FEATURES = N_PROGRAM_FEATURES + 1 + N_SCHEDULE_FEATURES + 1
 
@@ -393,7 +404,7 @@ def _device_inputs(nbits: int, n_inputs: int, seed: int):
     return bufs, {f"b{i}": (b.data_ptr(), nw) for i, b in enumerate(bufs)}
 
 
-CODEGEN_KEYS = ("warps", "min_blocks", "prefetch", "cut_adds", "layout", "chunk_words")
+CODEGEN_KEYS = ("warps", "min_blocks", "prefetch", "cut_adds", "layout", "chunk_words", "stages")
 
 
 def codegen_key(s: dict) -> tuple:

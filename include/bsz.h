@@ -80,6 +80,7 @@ typedef struct bsz_schedule {
                            2: as 1, with every input and output moved by TMA boxes of
                            chunk_words words x 32 threads through shared memory */
   int32_t chunk_words;  /* layout 2: 4 or 8 words per thread per box */
+  int32_t stages;       /* layout 2: 2 or 3 shared-memory stages of input boxes */
 } bsz_schedule;
 
 /* ---- library ---------------------------------------------------------- */

@@ -22,7 +22,7 @@ def test_candidate_space_is_the_product():
     m = 1
     for v in tuner.SEQ_AXES.values():
         m *= len(v)
-    n += m
+    n += m + len(tuner.TMA_CANDIDATES)
     assert len(c) == n == len(tuner.CANDIDATES)
     assert sum(1 for s in c if s["layout"] == 1) == m
     assert len({tuner.schedule_key(s) for s in c}) == n
