@@ -946,9 +946,16 @@ struct GenSeq {
     std::sort(mapped.begin(), mapped.end());
   }
   int box_bytes() const { return roww * 8 * 32; }
-  // shared memory per warp: `stages` boxes per mapped input + one per output
+  // output staging: two sets of boxes (a chunk's stores drain while the next
+  // chunk is computed) when they fit, else one
+  int out_stages() const {
+    const int two = warps * (stages * static_cast<int>(mapped.size()) + 2 * static_cast<int>(outs.size())) *
+                    box_bytes() + 1024;
+    return two <= 227 * 1024 ? 2 : 1;
+  }
+  // shared memory per warp: `stages` boxes per mapped input + staging boxes per output
   int smem_per_warp() const {
-    return (stages * static_cast<int>(mapped.size()) + static_cast<int>(outs.size())) * box_bytes();
+    return (stages * static_cast<int>(mapped.size()) + out_stages() * static_cast<int>(outs.size())) * box_bytes();
   }
   int smem_bytes() const { return warps * smem_per_warp() + 1024; }
 
@@ -1015,11 +1022,15 @@ struct GenSeq {
          ": \"=r\"(done) : \"r\"(mb), \"r\"((phase >> q) & 1u) : \"memory\");\n"
       << "        if (!__all_sync(~0u, done)) { if (lane == 0) atomicOr(A.fail, 2u); bail = true; break; }\n"
       << "        phase ^= 1u << q;\n        ++waited;\n      }\n"
-      << "      if (lane == 0) asm volatile(\"cp.async.bulk.wait_group.read 0;\" ::: \"memory\");\n"
+      // the staging set this chunk writes must have been read by its last
+      // stores: with two sets, the previous chunk's stores may still run
+      << "      if (lane == 0) asm volatile(\"cp.async.bulk.wait_group.read " << (out_stages() - 1)
+      << ";\" ::: \"memory\");\n"
       << "      __syncwarp();\n"
       << "      const long long w0 = s + (long long)ch * " << roww << ";\n"
       << "      unsigned char* ib = wb + q * " << nm * box << " + lane * " << rowb << ";\n"
-      << "      unsigned char* ob = wb + " << stages * nm * box << " + lane * " << rowb << ";\n"
+      << "      unsigned char* obase = wb + " << stages * nm * box << " + " << (out_stages() == 2 ? "(ch & 1) * " + std::to_string(no * box) : std::string("0")) << ";\n"
+      << "      unsigned char* ob = obase + lane * " << rowb << ";\n"
       << "      if (full) {\n"
       << "        if (" << (masked ? "w0 + " + std::to_string(roww) + " <= A.nw - 1" : std::string("true")) << ") {\n"
       << "#pragma unroll 1\n"
@@ -1065,8 +1076,8 @@ struct GenSeq {
       << "      if (lane == 0) {\n";
     for (int o = 0; o < no; ++o)
       s << "        asm volatile(\"cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];\" "
-           ":: \"l\"(&A.out_map[" << o << "]), \"r\"(0), \"r\"(ch), \"r\"((int)t0), \"r\"(smem_u32(wb + "
-        << stages * nm * box + o * box << ")) : \"memory\");\n";
+           ":: \"l\"(&A.out_map[" << o << "]), \"r\"(0), \"r\"(ch), \"r\"((int)t0), \"r\"(smem_u32(obase + "
+        << o * box << ")) : \"memory\");\n";
     s << "        asm volatile(\"cp.async.bulk.commit_group;\" ::: \"memory\");\n"
       << "      }\n      __syncwarp();\n    }\n"
       // after a bail-out: wait (bounded) for the loads still in flight
@@ -1564,10 +1575,17 @@ PartKernel part_kernel(const std::vector<Node>& nodes, const Part& p, int64_t N,
     pk.roww = g.roww;
     pk.smem = g.smem_bytes();
     pk.mapped = g.mapped;
-    BSZ_CU(drv().func_set_attribute(pk.c.fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, pk.smem));
-    if (drv().occupancy(&pk.tma_blocks_per_sm, pk.c.fn, sc.warps * 32, pk.smem) != CUDA_SUCCESS ||
-        pk.tma_blocks_per_sm < 1)
-      throw RuntimeError("fused: the TMA form does not fit on an SM (" + std::to_string(pk.smem) + " bytes)");
+    if (pk.smem > 227 * 1024 ||
+        drv().func_set_attribute(pk.c.fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, pk.smem) != CUDA_SUCCESS ||
+        drv().occupancy(&pk.tma_blocks_per_sm, pk.c.fn, sc.warps * 32, pk.smem) != CUDA_SUCCESS ||
+        pk.tma_blocks_per_sm < 1) {
+      // the boxes of this part do not fit in one SM's shared memory at this
+      // CTA size: the part takes the register form
+      Schedule s1 = sc;
+      s1.layout = 1;
+      s1.min_blocks = 1;
+      return part_kernel(nodes, p, N, s1, compile_ms);
+    }
   } else if (sc.layout == 1) {
     GenSeq g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0};
     pk.c = compile_source(g.source(), sc.warps * 32, compile_ms);
