@@ -846,10 +846,10 @@ struct GenSeq {
     const bool slow = mode != 'f';
     const std::string W = slow ? "w" : "(c + " + std::to_string(j) + ")";
     if (slow && masked) s << "      const u64 lm = (w == A.nw - 1) ? A.last_mask : ~0ull;\n";
-    for (auto& kv : in_idx) {
-      if (is_const(nodes[kv.first].op) && !slow) continue;
+    // every input and constant gets its value name (outputs and popcounts may
+    // name a constant directly: folding can reduce an output to ZERO)
+    for (auto& kv : in_idx)
       s << "      const u64 " << v(kv.first) << " = " << (slow ? ld(kv.first, "w") : fast_in(kv.first, j)) << ";\n";
-    }
     auto opnd = [&](int o) -> std::string {
       if (!slow && is_const(nodes[o].op)) return fast_in(o, j);
       return v(o);

@@ -127,3 +127,17 @@ def test_random_straight_line_programs_fused_matches_plain_and_oracle(ctx):
                 assert r.stream_int("outa", j) & mask == exp, (seed, mode, j)
             assert r.int("cnt") == want["cnt"], (seed, mode)
             assert r.stats["op_count"] == ops
+
+
+@pytest.mark.gpu
+def test_outputs_folded_to_constants_or_inputs(ctx):
+    """Folding can reduce an output to ZERO (a ^ a) or to an input; every form
+    must still store it and count its popcount."""
+    src = ("input stream a\ninput stream b\noutput stream z\noutput stream y\noutput stream w\n"
+           "output int nz\noutput int ny\noutput int nw\n"
+           "stream t = a ^ a\nz = t & b\ny = a\nstream s = a + b\nw = s << 1\n"
+           "nz = popcount(z)\nny = popcount(y)\nnw = popcount(w)\n")
+    nbits = (1 << 22) + 64 * 5
+    rng = np.random.default_rng(12)
+    inputs = {k: wl.random_words(rng, nbits) for k in "ab"}
+    run_both(ctx, src, nbits, inputs)
