@@ -719,10 +719,15 @@ struct GenSeq {
       for (size_t i = 0; i < part.outputs.size(); ++i) outs.push_back({part.outputs[i], static_cast<int>(i)});
     for (int n : part.order) in_part.insert(n);
     dyn.assign(nodes.size(), 0);
-    int64_t max_static = 0;
+    // Static dirt of nodes without an addition among their ancestors, in
+    // BITS: a value exact from bit B shifted left by k < 64 is exact from bit
+    // B + k (sdh keeps the word form, ceil(B / 64), which the warm-up checks
+    // and the run-time tracking of the other nodes use).
+    std::map<int, int64_t> sbits;
+    int64_t max_static_bits = 0;
     for (int n : part.order) {
       const Node& x = nodes[n];
-      auto d = [&](int o) -> int64_t { return (o >= 0 && sdh.count(o)) ? sdh[o] : 0; };
+      auto d = [&](int o) -> int64_t { return (o >= 0 && sbits.count(o)) ? sbits[o] : 0; };
       bool dy = x.op == NOp::Add;
       for (int o : {x.a, x.b})
         if (o >= 0 && dyn[o]) dy = true;
@@ -731,11 +736,11 @@ struct GenSeq {
         const int64_t ws = x.k / 64;
         if (in_part.count(x.a)) {
           if (ws > 0) throw RuntimeError("fused: shift of a temporary by 64 bits or more in a sequential part");
-          if (x.k > 0) { prev_src.insert(x.a); s = d(x.a) + 1; }
+          if (x.k > 0) { prev_src.insert(x.a); s = d(x.a) + x.k; }
         } else if (!is_const(nodes[x.a].op)) {
           if (ws == 0) {
-            // the previous word of an input is exact from the second warm-up word on
-            if (x.k > 0) { prev_src.insert(x.a); s = 1; }
+            // the previous word of an input is zero at the first warm-up word
+            if (x.k > 0) { prev_src.insert(x.a); s = x.k; }
           } else {
             off_slot[{x.a, -ws}] = 0;
             if (x.k % 64) off_slot[{x.a, -ws - 1}] = 0;
@@ -748,11 +753,12 @@ struct GenSeq {
       }
       dyn[n] = dy;
       if (!dy) {
-        sdh[n] = s;
-        max_static = std::max(max_static, s);
+        sbits[n] = s;
+        sdh[n] = (s + 63) / 64;
+        max_static_bits = std::max(max_static_bits, s);
       }
     }
-    warm = std::max<int64_t>(4, ((max_static + 2 + 3) / 4) * 4);
+    warm = std::max<int64_t>(4, (((max_static_bits + 63) / 64 + 2 + 3) / 4) * 4);
     int k = 0;
     for (auto& kv : off_slot) {
       kv.second = k++;
