@@ -34,7 +34,8 @@ class Schedule(ctypes.Structure):
     _fields_ = [("warps", ctypes.c_int32), ("range_steps", ctypes.c_int32),
                 ("ctas_per_sm", ctypes.c_int32), ("min_blocks", ctypes.c_int32),
                 ("prefetch", ctypes.c_int32), ("cut_adds", ctypes.c_int32), ("layout", ctypes.c_int32),
-                ("chunk_words", ctypes.c_int32), ("stages", ctypes.c_int32)]
+                ("chunk_words", ctypes.c_int32), ("stages", ctypes.c_int32),
+                ("unroll", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -220,6 +220,7 @@ int bsz_run_set_schedule(bsz_run* run, const bsz_schedule* s) {
     c.layout = s->layout;
     c.chunk_words = s->chunk_words;
     c.stages = s->stages;
+    c.unroll = s->unroll;
     executor(run).set_schedule(c);
   });
 }

@@ -144,6 +144,7 @@ void FusedBackend::set_schedule(const Schedule& s) {
   c.layout = std::max(0, std::min(c.layout, 2));
   c.chunk_words = c.chunk_words == 4 ? 4 : 8;
   c.stages = c.stages == 3 ? 3 : 2;
+  c.unroll = c.unroll ? 1 : 0;
   impl_->opt.sched = c;
 }
 
@@ -697,6 +698,7 @@ struct GenSeq {
   bool tma = false;
   int roww = 8;
   int stages = 2;
+  bool unroll_pairs = false;         // unroll a chunk's word pairs (more ILP, more code)
   std::vector<int> mapped;           // input indices (A.in order) that are read through boxes
   // batches: fixed argument positions and outputs that may be skipped (null)
   bool guard_outputs = false;
@@ -1039,7 +1041,7 @@ struct GenSeq {
       << "      unsigned char* ob = obase + lane * " << rowb << ";\n"
       << "      if (full) {\n"
       << "        if (" << (masked ? "w0 + " + std::to_string(roww) + " <= A.nw - 1" : std::string("true")) << ") {\n"
-      << "#pragma unroll 1\n"
+      << (unroll_pairs ? "#pragma unroll\n" : "#pragma unroll 1\n")
       << "          for (int pp = 0; pp < " << roww / 2 << "; ++pp) {\n"
       << "            const long long c = w0 + 2 * pp;\n"
       << "            const int po = (pp ^ sw) * 16;\n";
@@ -1529,6 +1531,7 @@ std::string graph_key(const std::vector<Node>& nodes, const std::vector<int>& or
   put(sc.layout);
   put(sc.chunk_words);
   put(sc.stages);
+  put(sc.unroll);
   return k;
 }
 
@@ -1575,6 +1578,7 @@ PartKernel part_kernel(const std::vector<Node>& nodes, const Part& p, int64_t N,
     g.tma = true;
     g.roww = sc.chunk_words == 4 ? 4 : 8;
     g.stages = sc.stages == 3 ? 3 : 2;
+    g.unroll_pairs = sc.unroll != 0;
     const std::string src = g.source();
     pk.c = compile_source(src, sc.warps * 32, compile_ms);
     pk.warm = g.warm;
@@ -1628,6 +1632,7 @@ bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& s
       g.tma = true;
       g.roww = sc.chunk_words == 4 ? 4 : 8;
       g.stages = sc.stages == 3 ? 3 : 2;
+      g.unroll_pairs = sc.unroll != 0;
       if (!is_compiled(g.source())) return false;
     } else if (sc.layout == 1) {
       GenSeq g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0};

@@ -81,6 +81,7 @@ typedef struct bsz_schedule {
                            chunk_words words x 32 threads through shared memory */
   int32_t chunk_words;  /* layout 2: 4 or 8 words per thread per box */
   int32_t stages;       /* layout 2: 2 or 3 shared-memory stages of input boxes */
+  int32_t unroll;       /* layout 2: 1 = the word pairs of a chunk are unrolled */
 } bsz_schedule;
 
 /* ---- library ---------------------------------------------------------- */
