@@ -195,7 +195,7 @@ k_shr(uint64_t* __restrict__ d, const uint64_t* __restrict__ a, int64_t ws, int 
 // written, by the one thread that writes it); partial overlaps are not
 // allowed.
 constexpr int kAddWarps = 8;
-constexpr int kAddSteps = 4;
+constexpr int kAddSteps = 2;
 constexpr int64_t kAddTile = kAddWarps * kAddSteps * 128;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
@@ -348,6 +348,9 @@ __device__ __forceinline__ void add_tile(AddTileRegs& r, AddShared& sh, const in
     wp &= sp;
   }
   if (lane == 0) sh.wagg[par][warp] = wg | (wp << 1);
+  // the ticket after next (its loads are issued while the next tile runs),
+  // drawn by warp 1, off warp 0's look-back path
+  if (threadIdx.x == 32) sh.ticket[par] = atomicAdd(&state[0], 1u);
   __syncthreads();
   if (warp == 0) {
     uint32_t tg = 0, tp = 1;
@@ -360,8 +363,6 @@ __device__ __forceinline__ void add_tile(AddTileRegs& r, AddShared& sh, const in
     uint32_t* status = state + 1;
     uint32_t cin = 0;
     if (lane == 0) {
-      // the ticket after next: its loads are issued while the next tile runs
-      sh.ticket[par] = atomicAdd(&state[0], 1u);
       if (tile != silent_tile) {
         if (tile == 0) {
           st_volatile(&status[0], kFlagInc | tg);
@@ -435,7 +436,7 @@ __device__ __forceinline__ void add_tile(AddTileRegs& r, AddShared& sh, const in
 // Forward progress: a CTA's tiles rise, so the lowest unresolved tile is
 // always some CTA's current tile, whose predecessor is resolved.
 template <bool VEC>
-__global__ void __launch_bounds__(kAddWarps * 32, 1)
+__global__ void __launch_bounds__(kAddWarps * 32, 2)
 k_add(uint64_t* d, const uint64_t* a, const uint64_t* b, int64_t n, uint64_t last_mask,
       uint32_t* __restrict__ state, uint32_t* __restrict__ err, int64_t silent_tile, int spin_limit) {
   __shared__ AddShared sh;
