@@ -178,25 +178,26 @@ k_shr(uint64_t* __restrict__ d, const uint64_t* __restrict__ a, int64_t ws, int 
 }
 
 // ---- add: single-pass carry scan ----------------------------------------
-// A CTA of kAddWarps warps owns one tile of kAddTile consecutive words.  Each
-// warp owns kAddSteps consecutive 128-word steps of it; in a step, lane l
-// owns the 4-word block at 4l: one 32-byte sector, a 256-bit load or store
-// per lane, so every warp access is one contiguous kilobyte.
+// The tile of the decoupled look-back is one WARP's: kAddSteps consecutive
+// 128-word steps (kAddTile words).  In a step, lane l owns the 4-word block
+// at 4l: one 32-byte sector, a 256-bit load or store per lane, so every warp
+// access is one contiguous kilobyte.  Warps are independent: each draws its
+// own tile ticket, publishes its aggregate as soon as its loads have landed
+// and resolves its carry in by look-back with no CTA barrier, so a warp
+// waiting on its predecessor holds up nobody else on the SM.
 //
 // Carry resolution inside a step: per block, generate g (the block sum with
 // no carry in overflowed) and propagate p (a ^ b is all ones over the block:
 // then, and only then, the carry out equals the carry in).  The carries into
 // the 32 blocks are the internal carries of the 32-bit addition
 // (G|P) + G + cin: carry into lane i = bit i of ((G|P)+G+cin) ^ P, carry out
-// = bit 32.  Across steps and warps the (g, p) pairs compose; across CTAs the
-// tile aggregate is published as soon as the tile's loads have landed and is
-// resolved by decoupled look-back (status word = flag | g | p<<1), with
-// bounded spins.  dst may be a or b exactly (each word is read before it is
-// written, by the one thread that writes it); partial overlaps are not
-// allowed.
-constexpr int kAddWarps = 8;
-constexpr int kAddSteps = 2;
-constexpr int64_t kAddTile = kAddWarps * kAddSteps * 128;
+// = bit 32.  Across steps the (g, p) pairs compose; across tiles the status
+// word is flag | g | p<<1, with bounded spins.  dst may be a or b exactly
+// (each word is read before it is written, by the one thread that writes
+// it); partial overlaps are not allowed.
+constexpr int kAddWarps = 8;   // warps per CTA (independent tiles)
+constexpr int kAddSteps = 4;
+constexpr int64_t kAddTile = kAddSteps * 128;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kFlagMask = 3u << 30;
@@ -288,129 +289,86 @@ __device__ __forceinline__ void inc4(uint64_t s[4], uint32_t c) {
   for (int i = 0; i < 4; ++i) s[i] = (static_cast<uint64_t>(r[2 * i + 1]) << 32) | r[2 * i];
 }
 
-// One tile's data in registers: 4 steps x a 4-word block of each operand.
-struct AddTileRegs {
-  uint64_t x[kAddSteps][4];
-  uint64_t y[kAddSteps][4];
-};
-
 template <bool VEC>
-__device__ __forceinline__ void load_tile(AddTileRegs& r, const uint64_t* a, const uint64_t* b, int64_t tile,
-                                          int64_t n) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t wbase = tile * kAddTile + static_cast<int64_t>(warp) * (kAddSteps * 128) + 4 * lane;
-#pragma unroll
-  for (int j = 0; j < kAddSteps; ++j) {
-    load4<VEC>(a, wbase + j * 128, n, r.x[j]);
-    load4<VEC>(b, wbase + j * 128, n, r.y[j]);
-  }
-}
-
-// Shared state of a CTA: per-warp aggregates and the tile's carry in, double
-// buffered by tile parity (a warp may still read the previous tile's while
-// another writes the next one's; two tiles apart a barrier separates them),
-// and the CTA's tickets.
-struct AddShared {
-  uint32_t wagg[2][kAddWarps];
-  uint32_t cin[2];
-  uint32_t ticket[2];
-};
-
-// Resolves and stores one tile held in `r` (its sums overwrite r.x).  Thread
-// 0 also draws the CTA's next ticket into sh.ticket[par].
-template <bool VEC>
-__device__ __forceinline__ void add_tile(AddTileRegs& r, AddShared& sh, const int par, uint64_t* d, int64_t n,
-                                         uint64_t last_mask, uint32_t* __restrict__ state,
-                                         uint32_t* __restrict__ err, int64_t silent_tile, int spin_limit,
-                                         const int64_t tile) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t wbase = tile * kAddTile + static_cast<int64_t>(warp) * (kAddSteps * 128) + 4 * lane;
+__global__ void __launch_bounds__(kAddWarps * 32)
+k_add(uint64_t* d, const uint64_t* a, const uint64_t* b, int64_t n, uint64_t last_mask,
+      uint32_t* __restrict__ state, uint32_t* __restrict__ err, int64_t silent_tile, int spin_limit) {
+  const int lane = threadIdx.x & 31;
+  uint32_t t32 = 0;
+  if (lane == 0) t32 = atomicAdd(&state[0], 1u);
+  const int64_t tile = __shfl_sync(0xffffffffu, t32, 0);
+  const int64_t wbase = tile * kAddTile + 4 * lane;
+  if (tile * kAddTile >= n) return;   // a whole warp past the end (grid rounding)
+  uint64_t sum[kAddSteps][4];
   uint32_t G[kAddSteps], P[kAddSteps];
+  {
+    uint64_t x[kAddSteps][4], y[kAddSteps][4];
 #pragma unroll
-  for (int j = 0; j < kAddSteps; ++j) {
-    const uint64_t q = (r.x[j][0] ^ r.y[j][0]) & (r.x[j][1] ^ r.y[j][1]) & (r.x[j][2] ^ r.y[j][2]) &
-                       (r.x[j][3] ^ r.y[j][3]);
-    uint64_t sum[4];
-    const uint32_t g = add4(sum, r.x[j], r.y[j]);
+    for (int j = 0; j < kAddSteps; ++j) {
+      load4<VEC>(a, wbase + j * 128, n, x[j]);
+      load4<VEC>(b, wbase + j * 128, n, y[j]);
+    }
 #pragma unroll
-    for (int i = 0; i < 4; ++i) r.x[j][i] = sum[i];
-    G[j] = __ballot_sync(0xffffffffu, g != 0);
-    // words past n are zero in both operands, so their blocks never propagate
-    P[j] = __ballot_sync(0xffffffffu, q == ~uint64_t(0));
+    for (int j = 0; j < kAddSteps; ++j) {
+      const uint32_t g = add4(sum[j], x[j], y[j]);
+      const uint64_t q = (x[j][0] ^ y[j][0]) & (x[j][1] ^ y[j][1]) & (x[j][2] ^ y[j][2]) & (x[j][3] ^ y[j][3]);
+      G[j] = __ballot_sync(0xffffffffu, g != 0);
+      // words past n are zero in both operands, so their blocks never propagate
+      P[j] = __ballot_sync(0xffffffffu, q == ~uint64_t(0));
+    }
   }
-  uint32_t wg = 0, wp = 1;
+  // the tile's aggregate over its steps (in word order)
+  uint32_t tg = 0, tp = 1;
 #pragma unroll
   for (int j = 0; j < kAddSteps; ++j) {
     const uint64_t z = static_cast<uint64_t>(G[j] | P[j]) + G[j];
     const uint32_t sg = static_cast<uint32_t>(z >> 32);
     const uint32_t sp = P[j] == 0xffffffffu;
-    wg = sg | (sp & wg);
-    wp &= sp;
+    tg = sg | (sp & tg);
+    tp &= sp;
   }
-  if (lane == 0) sh.wagg[par][warp] = wg | (wp << 1);
-  // the ticket after next (its loads are issued while the next tile runs),
-  // drawn by warp 1, off warp 0's look-back path
-  if (threadIdx.x == 32) sh.ticket[par] = atomicAdd(&state[0], 1u);
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t tg = 0, tp = 1;
-#pragma unroll
-    for (int w = 0; w < kAddWarps; ++w) {
-      const uint32_t g = sh.wagg[par][w] & 1u, p = sh.wagg[par][w] >> 1;
-      tg = g | (p & tg);
-      tp &= p;
-    }
+  uint32_t cin = 0;
+  if (lane == 0 && tile != silent_tile) {
     uint32_t* status = state + 1;
-    uint32_t cin = 0;
-    if (lane == 0) {
-      if (tile != silent_tile) {
-        if (tile == 0) {
-          st_volatile(&status[0], kFlagInc | tg);
-        } else {
-          st_volatile(&status[tile], kFlagAgg | tg | (tp << 1));
-          // walk back: (ag, ap) = composition of the tiles between j and this one
-          uint32_t ag = 0, ap = 1;
-          int64_t j = tile - 1;
-          int spins = 0;
-          while (true) {
-            const uint32_t v = ld_volatile(&status[j]);
-            const uint32_t f = v & kFlagMask;
-            if (f == 0) {
-              if (++spins > spin_limit) {
-                atomicOr(err, kErrLookbackTimeout);
-                cin = 0;
-                break;
-              }
-              __nanosleep(32);
-              continue;
-            }
-            if (f == kFlagInc) {
-              cin = ag | (ap & (v & 1u));
-              break;
-            }
-            const uint32_t g = v & 1u, p = (v >> 1) & 1u;
-            ag = ag | (ap & g);
-            ap &= p;
-            if (!ap) {   // the carry out of the walked range no longer depends on earlier tiles
-              cin = ag;
-              break;
-            }
-            --j;
-            spins = 0;
+    if (tile == 0) {
+      st_volatile(&status[0], kFlagInc | tg);
+    } else {
+      st_volatile(&status[tile], kFlagAgg | tg | (tp << 1));
+      // walk back: (ag, ap) = composition of the tiles between j and this one
+      uint32_t ag = 0, ap = 1;
+      int64_t j = tile - 1;
+      int spins = 0;
+      while (true) {
+        const uint32_t v = ld_volatile(&status[j]);
+        const uint32_t f = v & kFlagMask;
+        if (f == 0) {
+          if (++spins > spin_limit) {
+            atomicOr(err, kErrLookbackTimeout);
+            cin = 0;
+            break;
           }
-          __threadfence();
-          st_volatile(&status[tile], kFlagInc | (tg | (tp & cin)));
+          __nanosleep(32);
+          continue;
         }
+        if (f == kFlagInc) {
+          cin = ag | (ap & (v & 1u));
+          break;
+        }
+        const uint32_t g = v & 1u, p = (v >> 1) & 1u;
+        ag = ag | (ap & g);
+        ap &= p;
+        if (!ap) {   // the carry out of the walked range no longer depends on earlier tiles
+          cin = ag;
+          break;
+        }
+        --j;
+        spins = 0;
       }
-      sh.cin[par] = cin;
+      __threadfence();
+      st_volatile(&status[tile], kFlagInc | (tg | (tp & cin)));
     }
   }
-  __syncthreads();
-  uint32_t c = sh.cin[par];
-  for (int w = 0; w < warp; ++w) {
-    const uint32_t g = sh.wagg[par][w] & 1u, p = sh.wagg[par][w] >> 1;
-    c = g | (p & c);
-  }
+  uint32_t c = __shfl_sync(0xffffffffu, cin, 0);
 #pragma unroll
   for (int j = 0; j < kAddSteps; ++j) {
     const uint64_t z = static_cast<uint64_t>(G[j] | P[j]) + G[j] + c;
@@ -418,47 +376,14 @@ __device__ __forceinline__ void add_tile(AddTileRegs& r, AddShared& sh, const in
     c = static_cast<uint32_t>(z >> 32);
     const int64_t w = wbase + j * 128;
     if (w < n) {
-      inc4(r.x[j], (carries >> lane) & 1u);
+      inc4(sum[j], (carries >> lane) & 1u);
       if (w + 3 >= n - 1) {   // this block holds the last word
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-          if (w + i == n - 1) r.x[j][i] &= last_mask;
+          if (w + i == n - 1) sum[j][i] &= last_mask;
       }
-      store4<VEC>(d, w, n, r.x[j]);
+      store4<VEC>(d, w, n, sum[j]);
     }
-  }
-}
-
-// Persistent: each CTA draws tile tickets in order (first two at start, then
-// one per tile, during that tile's look-back) and keeps the next tile's
-// loads in flight while it resolves the current one, so neither the ticket
-// atomic nor the look-back sits between a tile's loads and the next ones.
-// Forward progress: a CTA's tiles rise, so the lowest unresolved tile is
-// always some CTA's current tile, whose predecessor is resolved.
-template <bool VEC>
-__global__ void __launch_bounds__(kAddWarps * 32, 2)
-k_add(uint64_t* d, const uint64_t* a, const uint64_t* b, int64_t n, uint64_t last_mask,
-      uint32_t* __restrict__ state, uint32_t* __restrict__ err, int64_t silent_tile, int spin_limit) {
-  __shared__ AddShared sh;
-  const int64_t tiles = (n + kAddTile - 1) / kAddTile;
-  if (threadIdx.x == 0) {
-    sh.ticket[0] = atomicAdd(&state[0], 1u);
-    sh.ticket[1] = atomicAdd(&state[0], 1u);
-  }
-  __syncthreads();
-  int64_t ta = sh.ticket[0], tb = sh.ticket[1];
-  AddTileRegs ra, rb;
-  if (ta < tiles) load_tile<VEC>(ra, a, b, ta, n);
-  while (ta < tiles) {
-    if (tb < tiles) load_tile<VEC>(rb, a, b, tb, n);
-    add_tile<VEC>(ra, sh, 0, d, n, last_mask, state, err, silent_tile, spin_limit, ta);
-    const int64_t tc = sh.ticket[0];
-    if (tb >= tiles) break;
-    if (tc < tiles) load_tile<VEC>(ra, a, b, tc, n);
-    add_tile<VEC>(rb, sh, 1, d, n, last_mask, state, err, silent_tile, spin_limit, tb);
-    const int64_t td = sh.ticket[1];
-    ta = tc;
-    tb = td;
   }
 }
 
@@ -574,14 +499,11 @@ static void launch_add_kernel(cudaStream_t stream, uint64_t* d, const uint64_t* 
   if (tiles > 0x7fffffff) throw std::invalid_argument("launch_add: stream too long");
   const bool vec = aligned32(d) && aligned32(a) && aligned32(b);
   auto k = vec ? k_add<true> : k_add<false>;
-  // persistent grid: the CTAs that stay resident (each loops over tiles)
-  int dev = 0, sms = 148, per_sm = 1;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kAddWarps * 32, 0) != cudaSuccess || per_sm < 1)
-    per_sm = 1;
-  const int64_t grid = std::min<int64_t>(tiles, static_cast<int64_t>(sms) * per_sm);
-  k<<<static_cast<unsigned>(grid), kAddWarps * 32, 0, stream>>>(d, a, b, n, last_mask, state, err,
-                                                                g_add_silent_tile, g_add_spin_limit);
+  // one warp per tile (each warp draws its own ticket)
+  const int64_t blocks = (tiles + kAddWarps - 1) / kAddWarps;
+  if (blocks > 0x7fffffff) throw std::invalid_argument("launch_add: stream too long");
+  k<<<static_cast<unsigned>(blocks), kAddWarps * 32, 0, stream>>>(d, a, b, n, last_mask, state, err,
+                                                                  g_add_silent_tile, g_add_spin_limit);
   check_launch();
 }
 
