@@ -181,10 +181,11 @@ k_shr(uint64_t* __restrict__ d, const uint64_t* __restrict__ a, int64_t ws, int 
 // The tile of the decoupled look-back is one WARP's: kAddSteps consecutive
 // 128-word steps (kAddTile words).  In a step, lane l owns the 4-word block
 // at 4l: one 32-byte sector, a 256-bit load or store per lane, so every warp
-// access is one contiguous kilobyte.  Warps are independent: each draws its
-// own tile ticket, publishes its aggregate as soon as its loads have landed
-// and resolves its carry in by look-back with no CTA barrier, so a warp
-// waiting on its predecessor holds up nobody else on the SM.
+// access is one contiguous kilobyte.  A CTA draws one ticket for kAddWarps
+// consecutive tiles; after that its warps are independent: each publishes its
+// aggregate as soon as its loads have landed and resolves its carry in by
+// look-back with no CTA barrier, so a warp waiting on its predecessor holds
+// up nobody else on the SM.
 //
 // Carry resolution inside a step: per block, generate g (the block sum with
 // no carry in overflowed) and propagate p (a ^ b is all ones over the block:
@@ -293,10 +294,13 @@ template <bool VEC>
 __global__ void __launch_bounds__(kAddWarps * 32)
 k_add(uint64_t* d, const uint64_t* a, const uint64_t* b, int64_t n, uint64_t last_mask,
       uint32_t* __restrict__ state, uint32_t* __restrict__ err, int64_t silent_tile, int spin_limit) {
+  // one ticket per CTA (same-address atomics serialize: one per warp would
+  // cost ~5 ns x 2^17 tiles); its warps take the CTA's kAddWarps tiles
+  __shared__ uint32_t s_ticket;
+  if (threadIdx.x == 0) s_ticket = atomicAdd(&state[0], 1u);
+  __syncthreads();
   const int lane = threadIdx.x & 31;
-  uint32_t t32 = 0;
-  if (lane == 0) t32 = atomicAdd(&state[0], 1u);
-  const int64_t tile = __shfl_sync(0xffffffffu, t32, 0);
+  const int64_t tile = static_cast<int64_t>(s_ticket) * kAddWarps + (threadIdx.x >> 5);
   const int64_t wbase = tile * kAddTile + 4 * lane;
   if (tile * kAddTile >= n) return;   // a whole warp past the end (grid rounding)
   uint64_t sum[kAddSteps][4];
