@@ -113,23 +113,29 @@ class Workload:
         return table.get(kname, float("nan"))
 
 
-def alu_roofline(prog, nbits: int, launch_ms: float, clocks) -> dict:
+def alu_roofline(prog, nbits: int, launch_ms: float, clocks, layout: int = 0) -> dict:
     """Integer-pipe roofline of a fused launch.  Algorithmic INT32 lane
-    operations per 64-bit word of the post-DCE DAG: 2 per AND/OR/XOR/NOT/
-    ANDNOT, 4 per shift (two funnel shifts and the neighbour word), 6 per ADD
-    (64-bit add, carry-generate compare, carry-in add).  Peak: 148 SMs x 128
-    INT32 lanes x the median SM clock seen while timing."""
+    instructions per 64-bit word of the post-DCE DAG, for the kernel form
+    that ran: 2 per AND/OR/XOR/NOT/ANDNOT (3-input LOP3 fusion can only make
+    that fewer), and per shift / ADD 4 / 6 in the warp form (neighbour word
+    through lane shuffles or ballots, carries by two ballots and a 32-bit add)
+    or 2 / 4 in the thread forms (two funnel shifts; a 4-instruction carry
+    chain).  Peak: the ALU pipe that executes them (logic, shift and integer
+    add: 16 lanes per SM sub-partition, 64 per SM; ncu counts the regex DAG's
+    thread-sequential kernel at 76.6 % of this pipe) x 148 SMs x the median SM
+    clock seen while timing."""
     from bitstreamzoo_b200 import tuner
     f = tuner.program_features(prog)
     n_ops = round(2 ** f[0] - 1)
-    per_word = n_ops * (2 * (f[1] + f[2]) + 4 * (f[3] + f[4] + f[6]) + 6 * f[5])
+    seq = layout >= 1
+    per_word = n_ops * (2 * (f[1] + f[2]) + (2 if seq else 4) * (f[3] + f[4] + f[6]) + (4 if seq else 6) * f[5])
     words = (nbits + 63) // 64
     mhz = (clocks or {}).get("sm_mhz") or 1965.0
-    peak = 148 * 128 * mhz * 1e6 / 1e12
+    peak = 148 * 64 * mhz * 1e6 / 1e12
     achieved = per_word * words / (launch_ms * 1e-3) / 1e12
     return {"bound": "int32", "dag_ops": n_ops, "int32_ops_per_word": per_word, "achieved": achieved,
             "peak": peak, "unit": "Tops/s", "frac": achieved / peak,
-            "peak_source": "nominal 148 SMs x 128 lanes x measured median SM clock"}
+            "peak_source": "ALU pipe: 148 SMs x 64 lanes x measured median SM clock"}
 
 
 DEFAULT_BITS = {"long_streams": 1 << 32, "regex_dag": 1 << 29, "matchstar": 1 << 24}
@@ -599,7 +605,7 @@ def measure_workload(E, workload: str, nbits: int, steps: int, warmup: int, main
                 "launch_ms": per_launch_ms,
                 "kernel_share": kv["ms"] / max(1e-9, sum(x["ms"] for x in prof.values()))}
         if kname.startswith("fused"):
-            roof["alu"] = alu_roofline(prog, nbits, per_launch_ms, main.get("clocks"))
+            roof["alu"] = alu_roofline(prog, nbits, per_launch_ms, main.get("clocks"), sched.get("layout", 0))
     res = {
         "metric": metric_name(workload), "value": main.get("value"), "unit": "GB/s",
         "ms_per_step": main.get("ms", float("nan")) / steps, "steps": steps, "warmup": warmup,
