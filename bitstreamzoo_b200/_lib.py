@@ -35,7 +35,7 @@ class Schedule(ctypes.Structure):
                 ("ctas_per_sm", ctypes.c_int32), ("min_blocks", ctypes.c_int32),
                 ("prefetch", ctypes.c_int32), ("cut_adds", ctypes.c_int32), ("layout", ctypes.c_int32),
                 ("chunk_words", ctypes.c_int32), ("stages", ctypes.c_int32),
-                ("unroll", ctypes.c_int32)]
+                ("unroll", ctypes.c_int32), ("shift_mul", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -221,6 +221,7 @@ int bsz_run_set_schedule(bsz_run* run, const bsz_schedule* s) {
     c.chunk_words = s->chunk_words;
     c.stages = s->stages;
     c.unroll = s->unroll;
+    c.shift_mul = s->shift_mul;
     executor(run).set_schedule(c);
   });
 }
@@ -560,6 +561,7 @@ bsz_batch* bsz_batch_create(bsz_ctx* ctx, bsz_program* const* programs, int n_pr
           s.layout = std::max(0, std::min(schedule->layout, 2));
           s.chunk_words = schedule->chunk_words == 4 ? 4 : 8;
           s.stages = schedule->stages == 3 ? 3 : 2;
+          s.shift_mul = schedule->shift_mul ? 1 : 0;
         }
         b->runner = std::make_unique<bsz::BatchRunner>(*ctx->dev, progs, std::move(inst), s);
         for (auto* p : b->progs) ++p->refs;

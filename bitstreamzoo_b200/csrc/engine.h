@@ -66,6 +66,7 @@ struct Schedule {
   int chunk_words = 8;    // layout 2: words per thread per box (4 or 8)
   int stages = 2;         // layout 2: shared-memory stages of input boxes (2 or 3)
   int unroll = 0;         // layout 2: 1 = each chunk's word pairs unrolled
+  int shift_mul = 0;      // layouts 1-2: 1 = shifts by multiply-adds (integer FMA pipe)
 };
 
 struct ExecOptions {

@@ -145,6 +145,7 @@ void FusedBackend::set_schedule(const Schedule& s) {
   c.chunk_words = c.chunk_words == 4 ? 4 : 8;
   c.stages = c.stages == 3 ? 3 : 2;
   c.unroll = c.unroll ? 1 : 0;
+  c.shift_mul = c.shift_mul ? 1 : 0;
   impl_->opt.sched = c;
 }
 
@@ -550,7 +551,7 @@ struct Gen {
     s << "typedef unsigned long long u64;\ntypedef unsigned int u32;\n"
       << "struct Args {\n  const u64* in[" << std::max(1, ni) << "];\n  u64* out[" << std::max(1, no)
       << "];\n  unsigned long long* slots;\n  unsigned int* fail;\n  long long nw;\n"
-      << "  long long range;\n  u64 last_mask;\n};\n";
+      << "  long long range;\n  u64 last_mask;\n  unsigned long long one;\n};\n";
     return s.str();
   }
 
@@ -699,6 +700,11 @@ struct GenSeq {
   int roww = 8;
   int stages = 2;
   bool unroll_pairs = false;         // unroll a chunk's word pairs (more ILP, more code)
+  // shifts of a word against its predecessor as integer multiply-adds by
+  // 2^k (the multiply pipe) instead of funnel shifts (the logic pipe, which
+  // bounds large DAGs); the multiplier comes from A.one so it stays a multiply
+  bool shift_mul = false;
+  std::set<int> mul_amounts;         // k % 32 of the shifts that use multipliers
   std::vector<int> mapped;           // input indices (A.in order) that are read through boxes
   // batches: fixed argument positions and outputs that may be skipped (null)
   bool guard_outputs = false;
@@ -891,7 +897,13 @@ struct GenSeq {
           const int bs = static_cast<int>(x.k % 64);
           std::string e;
           if (x.k == 0) e = a;
-          else if (ws == 0 && !is_const(nodes[x.a].op)) e = "fshl<" + std::to_string(bs) + ">(" + a + ", pv" + std::to_string(x.a) + ")";
+          else if (ws == 0 && !is_const(nodes[x.a].op)) {
+            if (shift_mul && bs != 32)
+              e = "fshl_m<" + std::to_string(bs) + ">(" + a + ", pv" + std::to_string(x.a) + ", pm" +
+                  std::to_string(bs % 32) + ")";
+            else
+              e = "fshl<" + std::to_string(bs) + ">(" + a + ", pv" + std::to_string(x.a) + ")";
+          }
           else if (is_const(nodes[x.a].op)) {
             // a constant shifted left: word w is the constant's word w - ws (and w - ws - 1)
             const std::string lo = ld(x.a, W + " - " + std::to_string(ws) + "ll");
@@ -976,7 +988,7 @@ struct GenSeq {
       << "struct ArgsT {\n  TMap in_map[" << std::max<size_t>(1, mapped.size()) << "];\n  TMap out_map["
       << std::max(1, no) << "];\n  const u64* in[" << std::max(1, ni) << "];\n  u64* out[" << std::max(1, no)
       << "];\n  unsigned long long* slots;\n  unsigned int* fail;\n  long long nw;\n  long long range;\n"
-      << "  u64 last_mask;\n  long long nfull;\n};\n"
+      << "  u64 last_mask;\n  long long nfull;\n  unsigned long long one;\n};\n"
       << "__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }\n";
     return s.str();
   }
@@ -1119,6 +1131,20 @@ struct GenSeq {
   // Device helpers shared by every thread-sequential kernel / device function.
   static std::string helpers() {
     std::ostringstream s;
+    s << "// funnel shift left by s in (0, 32) as multiplies, m = 2^s held in a register\n"
+         "// the compiler cannot fold: (hi << s) | (lo >> (32 - s)) = hi * m + mulhi(lo, m),\n"
+         "// two integer multiply-adds instead of a funnel shift on the logic pipe\n"
+         "__device__ __forceinline__ u32 fmul_funnel(u32 lo, u32 hi, u32 m) {\n"
+         "  u32 d;\n"
+         "  asm(\"{ .reg .u32 t; mul.hi.u32 t, %1, %3; mad.lo.u32 %0, %2, %3, t; }\" : \"=r\"(d) : \"r\"(lo), \"r\"(hi), \"r\"(m));\n"
+         "  return d;\n}\n"
+         "template <int K> __device__ __forceinline__ u64 fshl_m(u64 x, u64 p, u32 m) {\n"
+         "  const u32 xl = (u32)x, xh = (u32)(x >> 32), pl = (u32)p, ph = (u32)(p >> 32);\n"
+         "  u32 lo, hi;\n"
+         "  if constexpr (K < 32) { lo = fmul_funnel(ph, xl, m); hi = fmul_funnel(xl, xh, m); }\n"
+         "  else if constexpr (K == 32) { lo = ph; hi = xl; }\n"
+         "  else { lo = fmul_funnel(pl, ph, m); hi = fmul_funnel(ph, xl, m); }\n"
+         "  return ((u64)hi << 32) | lo;\n}\n";
     s << "template <int K> __device__ __forceinline__ u64 fshl(u64 x, u64 p) {\n"
          "  const u32 xl = (u32)x, xh = (u32)(x >> 32), pl = (u32)p, ph = (u32)(p >> 32);\n"
          "  u32 lo, hi;\n"
@@ -1175,6 +1201,15 @@ struct GenSeq {
     std::vector<int> adds;
     for (int n : part.order)
       if (nodes[n].op == NOp::Add) adds.push_back(n);
+    if (shift_mul) {
+      std::set<int> amounts;
+      for (int n : part.order) {
+        const Node& x = nodes[n];
+        if (x.op == NOp::Shl && x.k > 0 && x.k < 64 && x.k != 32 && !is_const(nodes[x.a].op))
+          amounts.insert(static_cast<int>(x.k % 32));
+      }
+      for (int k : amounts) s << "  const u32 pm" << k << " = (u32)(A.one << " << k << ");\n";
+    }
     for (int n : adds) s << "  u32 cy" << n << " = 0;\n";
     for (int n : prev_src) s << "  u64 pv" << n << " = 0;\n";
     for (size_t j = 0; j < part.pops.size(); ++j) s << "  u32 pc" << j << " = 0;\n";
@@ -1532,6 +1567,7 @@ std::string graph_key(const std::vector<Node>& nodes, const std::vector<int>& or
   put(sc.chunk_words);
   put(sc.stages);
   put(sc.unroll);
+  put(sc.shift_mul);
   return k;
 }
 
@@ -1579,6 +1615,7 @@ PartKernel part_kernel(const std::vector<Node>& nodes, const Part& p, int64_t N,
     g.roww = sc.chunk_words == 4 ? 4 : 8;
     g.stages = sc.stages == 3 ? 3 : 2;
     g.unroll_pairs = sc.unroll != 0;
+    g.shift_mul = sc.shift_mul != 0;
     const std::string src = g.source();
     pk.c = compile_source(src, sc.warps * 32, compile_ms);
     pk.warm = g.warm;
@@ -1598,6 +1635,7 @@ PartKernel part_kernel(const std::vector<Node>& nodes, const Part& p, int64_t N,
     }
   } else if (sc.layout == 1) {
     GenSeq g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0};
+    g.shift_mul = sc.shift_mul != 0;
     pk.c = compile_source(g.source(), sc.warps * 32, compile_ms);
     pk.warm = g.warm;
   } else {
@@ -1633,9 +1671,11 @@ bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& s
       g.roww = sc.chunk_words == 4 ? 4 : 8;
       g.stages = sc.stages == 3 ? 3 : 2;
       g.unroll_pairs = sc.unroll != 0;
+      g.shift_mul = sc.shift_mul != 0;
       if (!is_compiled(g.source())) return false;
     } else if (sc.layout == 1) {
       GenSeq g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0};
+      g.shift_mul = sc.shift_mul != 0;
       if (!is_compiled(g.source())) return false;
     } else {
       Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
@@ -1694,7 +1734,8 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
     // argument block, laid out as the generated struct
     const int ni = std::max<int>(1, static_cast<int>(p.inputs.size()));
     const int no = std::max<int>(1, static_cast<int>(p.outputs.size()));
-    std::vector<uint64_t> args(ni + no + 5, 0);
+    std::vector<uint64_t> args(ni + no + 6, 0);
+    args[ni + no + 5] = 1;   // `one`: a 1 the compiler cannot see (see GenSeq::shift_mul)
     for (size_t i = 0; i < p.inputs.size(); ++i) {
       const Node& x = nodes[p.inputs[i]];
       args[i] = x.buf ? reinterpret_cast<uint64_t>(x.buf->p) : 0;
@@ -1718,7 +1759,7 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
       const int nm = static_cast<int>(pk.mapped.size());
       const int nmp = std::max(1, nm), nop = std::max(1, static_cast<int>(p.outputs.size()));
       const size_t maps_bytes = 128 * static_cast<size_t>(nmp + nop);
-      targs.assign(((maps_bytes + 8 * (ni + no + 6)) + 63) / 64 * 64, 0);
+      targs.assign(((maps_bytes + 8 * (ni + no + 7)) + 63) / 64 * 64, 0);
       auto encode = [&](void* dst, const uint64_t* base) {
         cuuint64_t dims[3] = {static_cast<cuuint64_t>(R), static_cast<cuuint64_t>(range / R),
                               static_cast<cuuint64_t>(nfull)};
@@ -1744,6 +1785,7 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
       tail[ni + no + 3] = static_cast<uint64_t>(range);
       tail[ni + no + 4] = mask_for_bits(N);
       tail[ni + no + 5] = static_cast<uint64_t>(nfull);
+      tail[ni + no + 6] = 1;
     } else if (sc.layout >= 1) {
       // thread-sequential: one range of whole 4-word chunks per thread, at
       // least 16 warm-ups long; a persistent grid of what stays resident
@@ -2003,6 +2045,7 @@ BatchRunner::BatchRunner(Device& dev, const std::vector<const Program*>& progs,
     BatchProg bp = std::move(traced[k]);
     if (seq) {
       GenSeq g{bp.t.nodes, bp.part, 0, sched.warps, sched.min_blocks, true};
+      g.shift_mul = sched.shift_mul != 0;
       g.guard_outputs = true;
       g.in_index_override = &bp.in_index;
       g.outs_override = &bp.outs;
@@ -2041,7 +2084,7 @@ BatchRunner::BatchRunner(Device& dev, const std::vector<const Program*>& progs,
   src << "      default: break;\n    }\n  }\n}\n";
   m.kern = compile_source(src.str(), sched.warps * 32, &compile_ms, "bsz_batch");
   // 3. argument blocks (one Args per instance), slots and work items
-  const size_t stride = static_cast<size_t>(m.max_in + m.max_out + 5);
+  const size_t stride = static_cast<size_t>(m.max_in + m.max_out + 6);
   std::vector<uint64_t> args(stride * m.inst.size(), 0);
   BSZ_CUDA(cudaMalloc(&m.d_ctrl, 256));
   ++dev.n_mallocs;
@@ -2070,6 +2113,7 @@ BatchRunner::BatchRunner(Device& dev, const std::vector<const Program*>& progs,
     a[m.max_in + m.max_out + 2] = static_cast<uint64_t>(nw);
     a[m.max_in + m.max_out + 3] = static_cast<uint64_t>(range);
     a[m.max_in + m.max_out + 4] = mask_for_bits(bi.bitlength > 0 ? bi.bitlength : 64 * nw);
+    a[m.max_in + m.max_out + 5] = 1;
   }
   // items of one program together (warps then run the same device function,
   // so the instruction cache holds one DAG at a time), longest first within

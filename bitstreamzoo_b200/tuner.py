@@ -404,7 +404,8 @@ def _device_inputs(nbits: int, n_inputs: int, seed: int):
     return bufs, {f"b{i}": (b.data_ptr(), nw) for i, b in enumerate(bufs)}
 
 
-CODEGEN_KEYS = ("warps", "min_blocks", "prefetch", "cut_adds", "layout", "chunk_words", "stages", "unroll")
+CODEGEN_KEYS = ("warps", "min_blocks", "prefetch", "cut_adds", "layout", "chunk_words", "stages", "unroll",
+                "shift_mul")
 
 
 def codegen_key(s: dict) -> tuple:

@@ -82,6 +82,8 @@ typedef struct bsz_schedule {
   int32_t chunk_words;  /* layout 2: 4 or 8 words per thread per box */
   int32_t stages;       /* layout 2: 2 or 3 shared-memory stages of input boxes */
   int32_t unroll;       /* layout 2: 1 = the word pairs of a chunk are unrolled */
+  int32_t shift_mul;    /* layouts 1-2: 1 = shifts as integer multiply-adds (the multiply
+                           pipe) instead of funnel shifts (the logic pipe) */
 } bsz_schedule;
 
 /* ---- library ---------------------------------------------------------- */
