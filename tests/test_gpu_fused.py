@@ -25,7 +25,9 @@ import progen
 # 4-word rows; streams under 2^16 words take the register form instead)
 FORMS = [(bz.MODE_PLAIN, None), (bz.MODE_FUSED, {"layout": 0}), (bz.MODE_FUSED, {"layout": 1}),
          (bz.MODE_FUSED, {"layout": 2, "warps": 4, "min_blocks": 1}),
-         (bz.MODE_FUSED, {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1})]
+         (bz.MODE_FUSED, {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1}),
+         (bz.MODE_FUSED, {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1, "shift_mul": 1}),
+         (bz.MODE_FUSED, {"layout": 1, "warps": 4, "min_blocks": 1, "shift_mul": 1})]
 
 
 def run_both(ctx, src, nbits, inputs):
@@ -43,7 +45,8 @@ def run_both(ctx, src, nbits, inputs):
                 raise AssertionError(f"mode {mode} {sched} output {name}: first bad word {bad} of {got.size}")
         for name, v in ref_pops.items():
             assert r.int(name) == v, (mode, sched, name)
-        results[(mode, (sched or {}).get("layout"), (sched or {}).get("chunk_words"))] = r.stats
+        results[(mode, (sched or {}).get("layout"), (sched or {}).get("chunk_words"),
+                 (sched or {}).get("shift_mul"))] = r.stats
     return results
 
 
