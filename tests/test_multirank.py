@@ -55,3 +55,23 @@ def test_reference_arm_prints_one_line_under_two_ranks():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "reference"
+
+
+def test_streams_as_locals_keeps_the_operations():
+    """The reference runs in bench.py use the program with its output streams
+    as locals: the same operations and popcounts, no stream outputs."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from bitstreamzoo_b200 import workloads as wl
+    from oracle import pyoracle
+    for src, outs in ((wl.long_streams_src(), wl.LONG_OUTPUT_STREAMS),
+                      (wl.regex_dag_src(300, seed=3), [f"o{j}" for j in range(4)])):
+        loc = bench.streams_as_locals(src, outs)
+        assert "output stream" not in loc
+        nbits = 3000
+        ins = {n: (i * 0x9E3779B97F4A7C15 + 12345) % (1 << nbits) for i, n in
+               enumerate(pyoracle.parse(src)["inputs"])}
+        full, ops_full, _ = pyoracle.run_source(src, nbits, ins)
+        only, ops_loc, _ = pyoracle.run_source(loc, nbits, ins)
+        assert ops_full == ops_loc
+        assert {k: v for k, v in full.items() if k not in outs} == only
