@@ -65,6 +65,8 @@ def parse_args():
                     help="fused-kernel schedule: the autotuner's pick (every candidate of the 16-schedule "
                          "space timed before the timed region), the fastest of the shipped cost model's 4 "
                          "best predictions, the model's top-1 pick (no timing), or the default")
+    ap.add_argument("--schedule-json", default=None,
+                    help="a fixed fused-kernel schedule (JSON object over DEFAULT_SCHEDULE), e.g. for profiling")
     return ap.parse_args()
 
 
@@ -436,7 +438,10 @@ def measure_workload(E, workload: str, nbits: int, steps: int, warmup: int, main
     mode_of = {"fused": bz.MODE_FUSED, "plain": bz.MODE_PLAIN}
 
     sched, sched_src = dict(bz.DEFAULT_SCHEDULE), "default"
-    if schedule == "tuned":
+    if E.args.schedule_json:
+        sched.update(json.loads(E.args.schedule_json))
+        sched_src = "fixed (--schedule-json)"
+    elif schedule == "tuned":
         from bitstreamzoo_b200 import tuner
         ins = {k: (t.data_ptr(), nw) for k, t in dev_in.items()}
         sched = tuner.Autotuner(ctx).best(prog, W.src, nbits, ins)
