@@ -710,6 +710,8 @@ def measure_batched(E, instances: int, steps: int, warmup: int):
     # schedule: the warp form and the thread-sequential form, each timed over
     # 3 launches before the timed region; the faster one is measured
     cands = [dict(bz.DEFAULT_SCHEDULE), dict(bz.DEFAULT_SCHEDULE, layout=1, warps=8, min_blocks=1)]
+    if E.args.schedule_json:
+        cands = [dict(bz.DEFAULT_SCHEDULE, **json.loads(E.args.schedule_json))]
     tried = []
     build_s = 0.0
     for sc in cands:
@@ -780,8 +782,9 @@ def measure_batched(E, instances: int, steps: int, warmup: int):
                    "input_bytes": in_bytes, "output_bytes": out_bytes, "work_items": b.items,
                    "build_s": build_s, "l2": "inputs (all instances) far larger than L2",
                    "parallelism": f"replicas x{world}", "schedule": sched,
-                   "schedule_source": "faster of the warp and thread-sequential forms over 3 launches each: "
-                                      + ", ".join(f"layout {sc.get('layout', 0)} {ms:.2f} ms" for ms, sc in tried)},
+                   "schedule_source": ("--schedule-json" if E.args.schedule_json else
+                                       "faster of the warp and thread-sequential forms over 3 launches each: "
+                                       + ", ".join(f"layout {sc.get('layout', 0)} {ms:.2f} ms" for ms, sc in tried))},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": E.hbm,
                      "peak_source": E.hbm_src, "unit": "GB/s", "frac": achieved / E.hbm, "traffic": None,
                      "bytes_per_launch": in_bytes + out_bytes, "launch_ms": launch_ms},

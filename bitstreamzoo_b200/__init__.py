@@ -32,7 +32,7 @@ MODE_VM = 3
 MODES = {"plain": MODE_PLAIN, "fused": MODE_FUSED, "auto": MODE_AUTO, "vm": MODE_VM}
 
 DEFAULT_SCHEDULE = {"warps": 4, "range_steps": 64, "ctas_per_sm": 0, "min_blocks": 4,
-                    "prefetch": 1, "cut_adds": 0, "layout": 0, "chunk_words": 8,
+                    "prefetch": 1, "cut_adds": 0, "layout": 0, "chunk_words": 4,
                     "stages": 2, "unroll": 0, "shift_mul": 0}
 
 __all__ = ["Context", "Program", "Run", "B200Backend", "BszError", "MODE_PLAIN", "MODE_FUSED",

@@ -559,7 +559,7 @@ bsz_batch* bsz_batch_create(bsz_ctx* ctx, bsz_program* const* programs, int n_pr
           s.prefetch = schedule->prefetch;
           s.cut_adds = 0;
           s.layout = std::max(0, std::min(schedule->layout, 2));
-          s.chunk_words = schedule->chunk_words == 4 ? 4 : 8;
+          s.chunk_words = schedule->chunk_words == 8 ? 8 : 4;
           s.stages = schedule->stages == 3 ? 3 : 2;
           s.shift_mul = schedule->shift_mul ? 1 : 0;
         }

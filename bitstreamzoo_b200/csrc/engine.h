@@ -63,7 +63,7 @@ struct Schedule {
   int cut_adds = 0;       // 1: every addition ends a part (its result is materialized)
   int layout = 0;         // 0: warp ranges, lane = word; 1: thread-sequential ranges
                           // (register chunks); 2: thread-sequential ranges through TMA boxes
-  int chunk_words = 8;    // layout 2: words per thread per box (4 or 8)
+  int chunk_words = 4;    // layouts 1, 2: words per thread per chunk / box (4 or 8)
   int stages = 2;         // layout 2: shared-memory stages of input boxes (2 or 3)
   int unroll = 0;         // layout 2: 1 = each chunk's word pairs unrolled
   int shift_mul = 0;      // layouts 1-2: 1 = shifts by multiply-adds (integer FMA pipe)

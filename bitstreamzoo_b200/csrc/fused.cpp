@@ -142,7 +142,7 @@ void FusedBackend::set_schedule(const Schedule& s) {
   c.ctas_per_sm = std::max(-1, c.ctas_per_sm);
   c.min_blocks = std::max(1, std::min(c.min_blocks, 32));
   c.layout = std::max(0, std::min(c.layout, 2));
-  c.chunk_words = c.chunk_words == 4 ? 4 : 8;
+  c.chunk_words = c.chunk_words == 8 ? 8 : 4;
   c.stages = c.stages == 3 ? 3 : 2;
   c.unroll = c.unroll ? 1 : 0;
   c.shift_mul = c.shift_mul ? 1 : 0;
@@ -700,6 +700,7 @@ struct GenSeq {
   int roww = 8;
   int stages = 2;
   bool unroll_pairs = false;         // unroll a chunk's word pairs (more ILP, more code)
+  int reg_chunk = 4;                 // register form: words per chunk (4 or 8: 32- or 64-byte sectors)
   // shifts of a word against its predecessor as integer multiply-adds by
   // 2^k (the multiply pipe) instead of funnel shifts (the logic pipe, which
   // bounds large DAGs); the multiplier comes from A.one so it stays a multiply
@@ -1180,7 +1181,8 @@ struct GenSeq {
       s << "__device__ __noinline__ void " << fn_name
         << "(const Args* __restrict__ Ap, const long long s_item, const long long e_item, const int lane) {\n"
         << "  const Args& A = *Ap;\n"
-        << "  const long long L = (((e_item - s_item) + 31) / 32 + 3) / 4 * 4;\n"
+        << "  const long long L = (((e_item - s_item) + 31) / 32 + " << reg_chunk - 1 << ") / " << reg_chunk << " * "
+        << reg_chunk << ";\n"
         << "  const long long s = s_item + lane * L;\n"
         << "  const bool active = s < e_item;\n"
         << "  const long long e = min(s + L, e_item);\n";
@@ -1244,30 +1246,33 @@ struct GenSeq {
       emit_tma_body(s);
     } else {
     // ---- owned range
-    const int pad = static_cast<int>(fast_hi_pad) + (masked && fast_hi_pad == 3 ? 1 : 0);
+    const int CW = reg_chunk;
+    const int pad = static_cast<int>(fast_hi_pad) + (masked && fast_hi_pad == 3 ? 1 : 0) + (CW - 4);
     s << "  long long w = s;\n"
       << "  const long long fast_end = A.nw - 1 - " << pad << "ll;   // a fast chunk at c needs c <= fast_end\n"
       << "  while (w < e) {\n"
-      << "    if (w + 4 <= e && w >= " << fast_lo << "ll && w <= fast_end) {\n"
+      << "    if (w + " << CW << " <= e && w >= " << fast_lo << "ll && w <= fast_end) {\n"
       << "      const long long c = w;\n";
     for (auto& kv : in_idx) {
       if (is_const(nodes[kv.first].op)) continue;
       const std::string i = std::to_string(kv.second);
-      s << "      u64 c" << i << "_0, c" << i << "_1, c" << i << "_2, c" << i << "_3;\n"
-        << "      ld4(A.in[" << i << "] + c, c" << i << "_0, c" << i << "_1, c" << i << "_2, c" << i << "_3);\n";
+      for (int h = 0; h < CW; h += 4)
+        s << "      u64 c" << i << "_" << h << ", c" << i << "_" << h + 1 << ", c" << i << "_" << h + 2 << ", c" << i
+          << "_" << h + 3 << ";\n"
+          << "      ld4(A.in[" << i << "] + c + " << h << ", c" << i << "_" << h << ", c" << i << "_" << h + 1 << ", c"
+          << i << "_" << h + 2 << ", c" << i << "_" << h + 3 << ");\n";
     }
     for (auto& kv : off_slot) {
       const int n = kv.first.first;
       const int64_t base = slot_base(kv.first.second);
       const std::string sl = std::to_string(kv.second), i = std::to_string(in_idx.at(n));
-      s << "      u64 o" << sl << "_0, o" << sl << "_1, o" << sl << "_2, o" << sl << "_3, o" << sl << "_4, o" << sl
-        << "_5, o" << sl << "_6, o" << sl << "_7;\n"
-        << "      ld4(A.in[" << i << "] + c + (" << base << "ll), o" << sl << "_0, o" << sl << "_1, o" << sl << "_2, o"
-        << sl << "_3);\n"
-        << "      ld4(A.in[" << i << "] + c + (" << base + 4 << "ll), o" << sl << "_4, o" << sl << "_5, o" << sl
-        << "_6, o" << sl << "_7);\n";
+      for (int h = 0; h < CW + 4; h += 4)
+        s << "      u64 o" << sl << "_" << h << ", o" << sl << "_" << h + 1 << ", o" << sl << "_" << h + 2 << ", o" << sl
+          << "_" << h + 3 << ";\n"
+          << "      ld4(A.in[" << i << "] + c + (" << base + h << "ll), o" << sl << "_" << h << ", o" << sl << "_"
+          << h + 1 << ", o" << sl << "_" << h + 2 << ", o" << sl << "_" << h + 3 << ");\n";
     }
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < CW; ++j) {
       s << "      u64 ";
       bool first = true;
       for (auto& kv : outs) {
@@ -1284,10 +1289,11 @@ struct GenSeq {
     }
     for (auto& kv : outs) {
       const std::string o = std::to_string(kv.second);
-      s << "      " << guard(kv.second) << "st4(A.out[" << o << "] + c, r" << o << "_0, r" << o << "_1, r" << o << "_2, r" << o
-        << "_3);\n";
+      for (int h = 0; h < CW; h += 4)
+        s << "      " << guard(kv.second) << "st4(A.out[" << o << "] + c + " << h << ", r" << o << "_" << h << ", r" << o
+          << "_" << h + 1 << ", r" << o << "_" << h + 2 << ", r" << o << "_" << h + 3 << ");\n";
     }
-    s << "      w += 4;\n    } else {\n      {\n";
+    s << "      w += " << CW << ";\n    } else {\n      {\n";
     emit_word(s, 's', 0);
     emit_store_word(s);
     s << "      }\n      ++w;\n    }\n  }\n";
@@ -1636,6 +1642,7 @@ PartKernel part_kernel(const std::vector<Node>& nodes, const Part& p, int64_t N,
   } else if (sc.layout == 1) {
     GenSeq g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0};
     g.shift_mul = sc.shift_mul != 0;
+    g.reg_chunk = sc.chunk_words == 8 ? 8 : 4;
     pk.c = compile_source(g.source(), sc.warps * 32, compile_ms);
     pk.warm = g.warm;
   } else {
@@ -1676,6 +1683,7 @@ bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& s
     } else if (sc.layout == 1) {
       GenSeq g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0};
       g.shift_mul = sc.shift_mul != 0;
+      g.reg_chunk = sc.chunk_words == 8 ? 8 : 4;
       if (!is_compiled(g.source())) return false;
     } else {
       Gen g{nodes, p, N, sc.warps, sc.min_blocks, (N % 64) != 0, sc.prefetch != 0};
@@ -1793,8 +1801,9 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
                                                      : static_cast<int64_t>(dev.sm_count()) * per_sm * sc.warps * 32;
       const int64_t min_range = std::max<int64_t>(64, 16 * pk.warm);
       int64_t threads = std::max<int64_t>(1, std::min(threads_cap, (nw + min_range - 1) / min_range));
-      range = ((nw + threads - 1) / threads + 3) / 4 * 4;
-      range = std::min<int64_t>(std::max<int64_t>(range, 4), int64_t(1) << 25);   // per-thread popcounts fit u32
+      const int64_t cw = sc.chunk_words == 8 ? 8 : 4;
+      range = ((nw + threads - 1) / threads + cw - 1) / cw * cw;
+      range = std::min<int64_t>(std::max<int64_t>(range, cw), int64_t(1) << 25);   // per-thread popcounts fit u32
       const int64_t total = (nw + range - 1) / range;
       blocks = static_cast<int>((total + sc.warps * 32 - 1) / (sc.warps * 32));
     } else {
@@ -2046,6 +2055,7 @@ BatchRunner::BatchRunner(Device& dev, const std::vector<const Program*>& progs,
     if (seq) {
       GenSeq g{bp.t.nodes, bp.part, 0, sched.warps, sched.min_blocks, true};
       g.shift_mul = sched.shift_mul != 0;
+      g.reg_chunk = sched.chunk_words == 8 ? 8 : 4;
       g.guard_outputs = true;
       g.in_index_override = &bp.in_index;
       g.outs_override = &bp.outs;
@@ -2101,8 +2111,9 @@ BatchRunner::BatchRunner(Device& dev, const std::vector<const Program*>& progs,
     m.n_slots += static_cast<int64_t>(bp.t.pops.size());
     const int64_t nw = std::max<int64_t>(1, (bi.bitlength + 63) / 64);
     // work items: warp form, runs of 32-word steps; thread-sequential form,
-    // 32 lane ranges of whole 4-word chunks, each at least 16 warm-ups long
-    const int64_t range = seq ? 128 * ((std::max<int64_t>(64, 16 * bp.warm) + 3) / 4)
+    // 32 lane ranges of whole register chunks, each at least 16 warm-ups long
+    const int64_t cw = sched.chunk_words == 8 ? 8 : 4;
+    const int64_t range = seq ? 32 * cw * ((std::max<int64_t>(64, 16 * bp.warm) + cw - 1) / cw)
                               : 32 * std::max<int64_t>(sched.range_steps, (bp.warm / 32) * 8);
     for (int64_t s0 = 0; s0 < nw; s0 += range)
       items.push_back({static_cast<int32_t>(i), bi.program, s0, std::min(nw, s0 + range)});

@@ -106,7 +106,7 @@ def encode_schedule(s: dict) -> list[float]:
             float(s["prefetch"]), float(s["cut_adds"]),
             math.log2(32 * s["warps"] * max(1, s["min_blocks"])),
             float(layout >= 1), float(layout == 2),
-            math.log2(s.get("chunk_words", 8)) if layout == 2 else 0.0,
+            math.log2(s.get("chunk_words", 4)) if layout == 2 else 0.0,
             float(s.get("stages", 2)) if layout == 2 else 0.0]
 
 

@@ -79,7 +79,9 @@ typedef struct bsz_schedule {
                            (cross-word state in registers, 256-bit per-thread accesses);
                            2: as 1, with every input and output moved by TMA boxes of
                            chunk_words words x 32 threads through shared memory */
-  int32_t chunk_words;  /* layout 2: 4 or 8 words per thread per box */
+  int32_t chunk_words;  /* layout 1: 4 or 8 words per thread per register chunk (one or two
+                           256-bit accesses per stream); layout 2: 4 or 8 words per thread
+                           per box; any other value reads as 4 */
   int32_t stages;       /* layout 2: 2 or 3 shared-memory stages of input boxes */
   int32_t unroll;       /* layout 2: 1 = the word pairs of a chunk are unrolled */
   int32_t shift_mul;    /* layouts 1-2: 1 = shifts as integer multiply-adds (the multiply

@@ -67,7 +67,8 @@ def test_batched_mixed_programs_and_ragged_lengths(ctx):
 @pytest.mark.parametrize("schedule", [{"warps": 2, "range_steps": 32, "prefetch": 0},
                                       {"warps": 8, "range_steps": 256, "min_blocks": 2},
                                       {"layout": 1, "warps": 4, "min_blocks": 1},
-                                      {"layout": 1, "warps": 8, "min_blocks": 1}])
+                                      {"layout": 1, "warps": 8, "min_blocks": 1},
+                                      {"layout": 1, "chunk_words": 8, "warps": 4, "min_blocks": 1}])
 def test_batched_schedules(ctx, schedule):
     srcs, plan = wl.batched_plan(n_instances=40, n_dags=4, lo_log2=12, hi_log2=20, ops=200, seed=9)
     _run_batch(ctx, srcs, plan, seed=3, schedule=schedule)

@@ -24,10 +24,11 @@ import progen
 # register chunks, and thread-sequential ranges through TMA boxes (8- and
 # 4-word rows; streams under 2^16 words take the register form instead)
 FORMS = [(bz.MODE_PLAIN, None), (bz.MODE_FUSED, {"layout": 0}), (bz.MODE_FUSED, {"layout": 1}),
-         (bz.MODE_FUSED, {"layout": 2, "warps": 4, "min_blocks": 1}),
+         (bz.MODE_FUSED, {"layout": 2, "chunk_words": 8, "warps": 4, "min_blocks": 1}),
          (bz.MODE_FUSED, {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1}),
          (bz.MODE_FUSED, {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1, "shift_mul": 1}),
-         (bz.MODE_FUSED, {"layout": 1, "warps": 4, "min_blocks": 1, "shift_mul": 1})]
+         (bz.MODE_FUSED, {"layout": 1, "warps": 4, "min_blocks": 1, "shift_mul": 1}),
+         (bz.MODE_FUSED, {"layout": 1, "chunk_words": 8, "warps": 4, "min_blocks": 1})]
 
 
 def run_both(ctx, src, nbits, inputs):
