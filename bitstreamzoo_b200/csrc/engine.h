@@ -60,7 +60,10 @@ struct Schedule {
   int ctas_per_sm = 0;    // resident CTAs per SM; 0 = as many as the kernel's occupancy allows; -1 = no cap (one minimum-length range per warp)
   int min_blocks = 4;     // __launch_bounds__ minimum blocks (caps registers per thread)
   int prefetch = 1;       // issue the next step's loads before the current step's arithmetic
-  int cut_adds = 0;       // 1: every addition ends a part (its result is materialized)
+  int cut_adds = 0;       // carry scheme: 0, additions inside the generated kernels (speculative
+                          // carry state); 1, the same with every addition's result materialized;
+                          // 2, every addition run by the plain carry-scan kernel (decoupled
+                          // look-back) on materialized operands
   int layout = 0;         // 0: warp ranges, lane = word; 1: thread-sequential ranges
                           // (register chunks); 2: thread-sequential ranges through TMA boxes
   int chunk_words = 4;    // layouts 1, 2: words per thread per chunk / box (4 or 8)

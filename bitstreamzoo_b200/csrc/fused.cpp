@@ -142,6 +142,7 @@ void FusedBackend::set_schedule(const Schedule& s) {
   c.ctas_per_sm = std::max(-1, c.ctas_per_sm);
   c.min_blocks = std::max(1, std::min(c.min_blocks, 32));
   c.layout = std::max(0, std::min(c.layout, 2));
+  c.cut_adds = std::max(0, std::min(c.cut_adds, 2));
   c.chunk_words = c.chunk_words == 8 ? 8 : 4;
   c.stages = c.stages == 3 ? 3 : 2;
   c.unroll = c.unroll ? 1 : 0;
@@ -157,6 +158,8 @@ struct Part {
   std::vector<int> inputs;                    // materialized nodes read (Buf or earlier part)
   std::vector<int> outputs;                   // nodes to store
   std::vector<std::pair<int, int64_t>> pops;  // (node, slot)
+  bool lookback_add = false;                  // one addition of materialized operands, run by
+                                              // the plain carry-scan kernel (decoupled look-back)
 };
 
 struct Gen {
@@ -1453,8 +1456,13 @@ Compiled compile_source(const std::string& src, int block_threads, double* compi
 // Splits a segment into parts: a node that reads a temporary through a right
 // shift, or through a left shift of 64 * shl_cut_words bits or more (2048 in
 // the warp form, 64 in the thread-sequential form), starts a later part, and
-// that temporary becomes an output of its own part.
-std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg, bool cut_adds,
+// that temporary becomes an output of its own part.  Carry schemes
+// (cut_adds): 0, every addition inside the generated kernel (speculative
+// carry state); 1, the same, with every addition's result materialized; 2,
+// every addition of two streams is a part of its own run by the plain
+// carry-scan kernel (decoupled look-back), its operands and result
+// materialized.
+std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg, int cut_adds,
                         int64_t shl_cut_words = 32) {
   std::map<int, int> level;
   std::set<int> computed(seg.order.begin(), seg.order.end());
@@ -1466,7 +1474,7 @@ std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg, bool
       if (o < 0 || !computed.count(o)) continue;
       int l = level[o];
       bool cut = (x.op == NOp::Shr) || (x.op == NOp::Shl && x.k / 64 >= shl_cut_words) ||
-                 (cut_adds && nodes[o].op == NOp::Add);
+                 (cut_adds && nodes[o].op == NOp::Add) || (cut_adds == 2 && x.op == NOp::Add);
       if (cut) {
         cut_src.insert(o);
         l += 1;
@@ -1479,7 +1487,14 @@ std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg, bool
   for (auto& kv : level) max_lv = std::max(max_lv, kv.second);
   std::vector<Part> parts(max_lv + 1);
   std::set<int> seg_out(seg.outputs.begin(), seg.outputs.end());
-  for (int n : seg.order) parts[level[n]].order.push_back(n);
+  std::vector<std::vector<int>> adds_at(max_lv + 1);
+  for (int n : seg.order) {
+    // carry scheme 2: an addition reads only materialized operands and is
+    // read only from memory, so it shares its level with nothing it depends
+    // on or that depends on it, and leaves that level's kernel
+    if (cut_adds == 2 && nodes[n].op == NOp::Add) adds_at[level[n]].push_back(n);
+    else parts[level[n]].order.push_back(n);
+  }
   for (int L = 0; L <= max_lv; ++L) {
     Part& p = parts[L];
     std::set<int> in_this(p.order.begin(), p.order.end());
@@ -1501,7 +1516,12 @@ std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg, bool
     p.inputs.assign(ins.begin(), ins.end());
   }
   // pops go to the part that computes their node (or part 0 for inputs)
+  std::map<int, std::vector<std::pair<int, int64_t>>> add_pops;
   for (auto& pp : seg.pops) {
+    if (cut_adds == 2 && computed.count(pp.first) && nodes[pp.first].op == NOp::Add) {
+      add_pops[pp.first].push_back(pp);
+      continue;
+    }
     int L = computed.count(pp.first) ? level[pp.first] : 0;
     Part& p = parts[L];
     p.pops.push_back(pp);
@@ -1509,7 +1529,21 @@ std::vector<Part> split(const std::vector<Node>& nodes, const Segment& seg, bool
         std::find(p.inputs.begin(), p.inputs.end(), pp.first) == p.inputs.end())
       p.inputs.push_back(pp.first);
   }
-  return parts;
+  if (cut_adds != 2) return parts;
+  std::vector<Part> out;
+  for (int L = 0; L <= max_lv; ++L) {
+    for (int n : adds_at[L]) {
+      Part a;
+      a.lookback_add = true;
+      a.order = {n};
+      a.inputs = {nodes[n].a, nodes[n].b};
+      a.outputs = {n};
+      a.pops = add_pops[n];
+      out.push_back(std::move(a));
+    }
+    out.push_back(std::move(parts[L]));
+  }
+  return out;
 }
 
 }  // namespace
@@ -1664,9 +1698,9 @@ bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& s
     if (plan_cache().count(graph_key(nodes, seg.order, seg.inputs, seg.outputs, seg.pops, (N % 64) != 0, sc)))
       return true;
   }
-  std::vector<Part> parts = split(nodes, seg, sc.cut_adds != 0, sc.layout >= 1 ? 1 : 32);
+  std::vector<Part> parts = split(nodes, seg, sc.cut_adds, sc.layout >= 1 ? 1 : 32);
   for (Part& p : parts) {
-    if (p.order.empty() && p.pops.empty()) continue;
+    if ((p.order.empty() && p.pops.empty()) || p.lookback_add) continue;
     if (p.inputs.size() > kMaxInputs) return false;
     {
       std::lock_guard<std::mutex> lk(g_part_mu);
@@ -1721,10 +1755,10 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
   }
   if (!plan) {
     auto np = std::make_shared<SegPlan>();
-    for (Part& p : split(nodes, seg, sc.cut_adds != 0, sc.layout >= 1 ? 1 : 32)) {
+    for (Part& p : split(nodes, seg, sc.cut_adds, sc.layout >= 1 ? 1 : 32)) {
       if (p.order.empty() && p.pops.empty()) continue;
       if (p.inputs.size() > kMaxInputs) throw RuntimeError("fused: too many inputs in one segment");
-      np->kernels.push_back(part_kernel(nodes, p, N, sc, compile_ms));
+      np->kernels.push_back(p.lookback_add ? PartKernel{} : part_kernel(nodes, p, N, sc, compile_ms));
       np->parts.push_back(std::move(p));
     }
     std::lock_guard<std::mutex> lk(g_plan_mu);
@@ -1739,6 +1773,30 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
     // outputs
     for (int n : p.outputs)
       if (!nodes[n].buf) nodes[n].buf = dev.alloc_stream(nw);
+    if (p.lookback_add) {
+      // carry scheme 2: the plain single-pass carry scan on materialized
+      // operands (a constant operand is filled into a temporary first)
+      const Node& x = nodes[p.order[0]];
+      const uint64_t lm = mask_for_bits(N);
+      BufRef tmp[2];
+      const uint64_t* opnd[2];
+      for (int k = 0; k < 2; ++k) {
+        const Node& y = nodes[k == 0 ? x.a : x.b];
+        if (y.buf) {
+          opnd[k] = y.buf->p;
+        } else if (is_const(y.op)) {
+          tmp[k] = dev.alloc_stream(nw);
+          const uint64_t val = y.op == NOp::Zero ? 0 : ~uint64_t(0);
+          launch_fill(dev, tmp[k]->p, nw, val, y.op == NOp::OnesMask ? lm : val);
+          opnd[k] = tmp[k]->p;
+        } else {
+          throw RuntimeError("fused: an addition operand without a buffer");
+        }
+      }
+      launch_add(dev, nodes[p.order[0]].buf->p, opnd[0], opnd[1], nw, lm);
+      for (auto& pp : p.pops) launch_popcount(dev, nodes[pp.first].buf->p, nw, d_slots + pp.second);
+      continue;
+    }
     // argument block, laid out as the generated struct
     const int ni = std::max<int>(1, static_cast<int>(p.inputs.size()));
     const int no = std::max<int>(1, static_cast<int>(p.outputs.size()));

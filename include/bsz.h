@@ -73,7 +73,11 @@ typedef struct bsz_schedule {
                            persistent cap: one minimum-length range per warp */
   int32_t min_blocks;   /* launch-bounds minimum blocks per SM (caps registers) */
   int32_t prefetch;     /* 1: load the next 32-word step before computing this one */
-  int32_t cut_adds;     /* 1: materialize every addition (one kernel per addition level) */
+  int32_t cut_adds;     /* carry scheme: 0, additions inside the fused kernels (speculative
+                           carry state, exact re-run if unproven); 1, the same with every
+                           addition's result materialized (one kernel per addition level);
+                           2, every addition of two streams run by the plain single-pass
+                           carry-scan kernel (decoupled look-back) on materialized operands */
   int32_t layout;       /* 0: each warp walks a word range, lane = word (cross-word state by
                            ballots and shuffles); 1: each thread walks its own word range
                            (cross-word state in registers, 256-bit per-thread accesses);
