@@ -109,11 +109,28 @@ struct Compiled {
   int blocks_per_sm = 1;   // occupancy of the compiled kernel at its block size
 };
 
-// Process-wide cache of compiled kernels keyed by generated source.
+// Process-wide cache of compiled kernels keyed by a 128-bit digest of the
+// generated source (two independent 64-bit hashes and the length), not the
+// source itself: a tuning run holds tens of thousands of kernels whose
+// sources are hundreds of kilobytes each.
 std::mutex g_cache_mu;
-std::map<std::string, Compiled>& cache() {
-  static std::map<std::string, Compiled> c;
+std::unordered_map<std::string, Compiled>& cache() {
+  static std::unordered_map<std::string, Compiled> c;
   return c;
+}
+
+std::string src_digest(const std::string& src) {
+  uint64_t h1 = 1469598103934665603ull, h2 = 0x9E3779B97F4A7C15ull;
+  for (char ch : src) {
+    const uint64_t c = static_cast<unsigned char>(ch);
+    h1 = (h1 ^ c) * 1099511628211ull;   // FNV-1a
+    h2 = (h2 + c + 1) * 0xff51afd7ed558ccdull;
+    h2 ^= h2 >> 29;
+  }
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%016llx%016llx:%zu", static_cast<unsigned long long>(h1),
+                static_cast<unsigned long long>(h2), src.size());
+  return buf;
 }
 
 bool is_const(NOp op) { return op == NOp::Zero || op == NOp::OnesMask || op == NOp::AllOnes; }
@@ -1388,7 +1405,7 @@ void disk_cache_store(const std::string& src, const std::string& cubin) {
 bool is_compiled(const std::string& src) {
   {
     std::lock_guard<std::mutex> lk(g_cache_mu);
-    if (cache().count(src)) return true;
+    if (cache().count(src_digest(src))) return true;
   }
   const std::string dir = cache_dir();
   if (dir.empty()) return false;
@@ -1401,9 +1418,10 @@ bool is_compiled(const std::string& src) {
 
 Compiled compile_source(const std::string& src, int block_threads, double* compile_ms,
                         const char* kernel = "bsz_fused") {
+  const std::string digest = src_digest(src);
   {
     std::lock_guard<std::mutex> lk(g_cache_mu);
-    auto it = cache().find(src);
+    auto it = cache().find(digest);
     if (it != cache().end()) return it->second;
   }
   auto t0 = std::chrono::high_resolution_clock::now();
@@ -1449,7 +1467,7 @@ Compiled compile_source(const std::string& src, int block_threads, double* compi
   if (compile_ms)
     *compile_ms += std::chrono::duration<double, std::milli>(std::chrono::high_resolution_clock::now() - t0).count();
   std::lock_guard<std::mutex> lk(g_cache_mu);
-  cache()[src] = c;
+  cache()[digest] = c;
   return c;
 }
 

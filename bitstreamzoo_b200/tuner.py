@@ -4,7 +4,10 @@ The fused backend's generated kernels take a schedule (``bsz_schedule`` in
 include/bsz.h): CTA size in warps, the launch-bounds minimum of resident
 CTAs per SM (which caps registers per thread), an occupancy cap, the minimum
 run of 32-word steps a warp owns, software prefetch of the next step's
-loads, and whether ripple adds end a kernel.  The best setting depends on
+loads, the kernel form (warp ranges, thread ranges in registers, thread
+ranges through TMA boxes) with its chunk size and shift instructions, and
+the carry scheme (speculative carry state inside the generated kernels, or
+every addition by the plain look-back carry scan).  The best setting depends on
 the DAG (op mix, shift distances, carry chains, live temporaries) and on the
 stream length, so it is searched, not fixed:
 
@@ -53,20 +56,35 @@ LAUNCH_AXES = {"ctas_per_sm": (0, 2)}
 # The thread-sequential form (layout 1): its register-resident chunk needs
 # the full register file (min_blocks 1; at min_blocks 2 the 2,000-op regex
 # DAG spills and runs 2x slower), and prefetch / range_steps do not apply.
+# Its axes: 4- or 8-word register chunks, and shifts as funnel shifts (ALU
+# pipe) or as integer multiply-adds (multiply pipe).
 SEQ_AXES = {"layout": (1,), "warps": (4, 8), "min_blocks": (1,), "prefetch": (0,), "cut_adds": (0,),
-            "ctas_per_sm": (0,)}
-# The TMA form (layout 2): 4-word rows for 8 warps per CTA (2 or 3 stages),
-# 4-word rows for 4 warps (two CTAs per SM); 8-word rows leave room for only
-# 4 warps per SM and measured 1.7x slower on the regex DAG, so they are out.
+            "ctas_per_sm": (0,), "chunk_words": (4, 8), "shift_mul": (0, 1)}
+# The TMA form (layout 2): 4-word rows for 8 warps per CTA (2 or 3 stages,
+# funnel or multiply shifts), 4-word rows for 4 warps (two CTAs per SM);
+# 8-word rows leave room for only 4 warps per SM and measured 1.7x slower on
+# the regex DAG, so they are out.
 TMA_CANDIDATES = [{"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1, "prefetch": 0, "stages": 2},
                   {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1, "prefetch": 0, "stages": 3},
-                  {"layout": 2, "chunk_words": 4, "warps": 4, "min_blocks": 1, "prefetch": 0, "stages": 2}]
+                  {"layout": 2, "chunk_words": 4, "warps": 4, "min_blocks": 1, "prefetch": 0, "stages": 2},
+                  {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1, "prefetch": 0, "stages": 2,
+                   "shift_mul": 1}]
+# The carry-scheme axis: every addition run by the plain single-pass
+# carry scan (decoupled look-back) on materialized operands, the rest of
+# the DAG in generated kernels of each form (cut_adds 2), against the
+# speculative carry state of every other candidate.
+CARRY_CANDIDATES = [{"layout": 0, "warps": 4, "min_blocks": 4, "prefetch": 1, "cut_adds": 2},
+                    {"layout": 1, "warps": 8, "min_blocks": 1, "prefetch": 0, "cut_adds": 2},
+                    {"layout": 1, "warps": 4, "min_blocks": 1, "prefetch": 0, "chunk_words": 8, "cut_adds": 2},
+                    {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1, "prefetch": 0, "stages": 2,
+                     "cut_adds": 2}]
 
 
 def candidate_space(codegen=None, launch=None, seq=None) -> list[dict]:
     """Cartesian product of the axes, each a full schedule dict: the warp
-    form's codegen x launch axes, then the thread-sequential form's axes
-    (``seq``; pass an empty dict to leave that form out)."""
+    form's codegen x launch axes, then the thread-sequential form's axes,
+    the TMA form's candidates and the look-back carry scheme's (``seq``;
+    pass an empty dict to leave all but the warp form out)."""
     codegen = codegen or CODEGEN_AXES
     launch = launch or LAUNCH_AXES
     seq = SEQ_AXES if seq is None else seq
@@ -81,7 +99,7 @@ def candidate_space(codegen=None, launch=None, seq=None) -> list[dict]:
             s = dict(DEFAULT_SCHEDULE)
             s.update(dict(zip(list(seq), vals)))
             out.append(s)
-        for t in TMA_CANDIDATES:
+        for t in TMA_CANDIDATES + CARRY_CANDIDATES:
             s = dict(DEFAULT_SCHEDULE)
             s.update(t)
             out.append(s)
@@ -96,21 +114,26 @@ def schedule_key(s: dict) -> tuple:
 
 
 def encode_schedule(s: dict) -> list[float]:
-    """Schedule features (11): log2 warps, log2 min_blocks, occupancy cap
-    (0 = none), log2 range_steps, prefetch, cut_adds, log2 threads x
-    min_blocks (the register cap's denominator), thread-sequential form,
-    TMA form, log2 chunk words and stages (TMA form; 0 otherwise)."""
+    """Schedule features (13): log2 warps, log2 min_blocks, occupancy cap
+    (0 = none), log2 range_steps, prefetch, additions materialized (carry
+    scheme 1), log2 threads x min_blocks (the register cap's denominator),
+    thread-sequential form, TMA form, log2 chunk words (thread forms), stages
+    (TMA form), multiply-form shifts (thread forms) and look-back additions
+    (carry scheme 2); 0 where a knob does not apply."""
     layout = int(s.get("layout", 0))
+    cut = int(s.get("cut_adds", 0))
     return [math.log2(s["warps"]), math.log2(max(1, s["min_blocks"])),
             math.log2(1 + max(0, s["ctas_per_sm"])), math.log2(max(1, s["range_steps"])),
-            float(s["prefetch"]), float(s["cut_adds"]),
+            float(s["prefetch"]), float(cut == 1),
             math.log2(32 * s["warps"] * max(1, s["min_blocks"])),
             float(layout >= 1), float(layout == 2),
-            math.log2(s.get("chunk_words", 4)) if layout == 2 else 0.0,
-            float(s.get("stages", 2)) if layout == 2 else 0.0]
+            math.log2(s.get("chunk_words", 4)) if layout >= 1 else 0.0,
+            float(s.get("stages", 2)) if layout == 2 else 0.0,
+            float(s.get("shift_mul", 0)) if layout >= 1 else 0.0,
+            float(cut == 2)]
 
 
-N_SCHEDULE_FEATURES = 11
+N_SCHEDULE_FEATURES = 13
 N_PROGRAM_FEATURES = 15
 N_FEATURES = N_PROGRAM_FEATURES + 1 + N_SCHEDULE_FEATURES + 1
 
@@ -413,14 +436,17 @@ def codegen_key(s: dict) -> tuple:
     return tuple(int(s.get(k, DEFAULT_SCHEDULE[k])) for k in CODEGEN_KEYS)
 
 
-def precompile(srcs, candidates=None, nbits: int = 1 << 22, threads: int | None = None, log=None) -> float:
+def precompile(srcs, candidates=None, nbits: int = 1 << 22, threads: int | None = None, log=None,
+               only=None) -> float:
     """Compiles the fused kernels of every (program, code variant) pair
     ahead of timing, in parallel host threads, each with its own context
     (NVRTC runs on the host; the process-wide kernel cache then serves the
     timing runs).  Kernels do not depend on the stream length beyond its
     word alignment, so one short run per pair (``nbits``, a multiple of 64
-    long enough for every form) compiles what every length uses.  Returns
-    the wall seconds."""
+    long enough for every form) compiles what every length uses.  ``only``
+    (one set of :func:`codegen_key` values per source, or None for all)
+    limits a source to the variants that will be timed.  Returns the wall
+    seconds."""
     import concurrent.futures as cf
     import threading
     import time as _time
@@ -431,7 +457,8 @@ def precompile(srcs, candidates=None, nbits: int = 1 << 22, threads: int | None 
     reps = {}
     for s in candidates:
         reps.setdefault(codegen_key(s), s)
-    jobs = [(src, s) for src in srcs for s in reps.values()]
+    jobs = [(src, s) for i, src in enumerate(srcs) for k, s in reps.items()
+            if only is None or only[i] is None or k in only[i]]
     local = threading.local()
     ctxs = []
     lock = threading.Lock()
@@ -503,7 +530,8 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candida
         k = max(1, int(round(sample_frac * len(variants))))
         chosen_by.append({variants[j] for j in rng.choice(len(variants), size=k, replace=False)})
     if precompile_threads:
-        t_pc = precompile(train_srcs + test_srcs, candidates, threads=precompile_threads, log=log)
+        t_pc = precompile(train_srcs + test_srcs, candidates, threads=precompile_threads, log=log,
+                          only=chosen_by + [None] * len(test_srcs))
         if log:
             log(f"precompiled in {t_pc:.0f}s")
     t0 = _time.time()
@@ -582,6 +610,8 @@ def main(argv=None):
 
     from . import Context
 
+    # tens of thousands of kernels: keep them in this process, not on disk
+    os.environ.setdefault("BSZ_KERNEL_CACHE", "off")
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=None)
     ap.add_argument("--json", default=None)

@@ -22,9 +22,10 @@ def test_candidate_space_is_the_product():
     m = 1
     for v in tuner.SEQ_AXES.values():
         m *= len(v)
-    n += m + len(tuner.TMA_CANDIDATES)
-    assert len(c) == n == len(tuner.CANDIDATES)
-    assert sum(1 for s in c if s["layout"] == 1) == m
+    n += m + len(tuner.TMA_CANDIDATES) + len(tuner.CARRY_CANDIDATES)
+    assert len(c) == n == len(tuner.CANDIDATES) == 32
+    assert sum(1 for s in c if s["layout"] == 1 and s["cut_adds"] == 0) == m
+    assert sum(1 for s in c if s["cut_adds"] == 2) == len(tuner.CARRY_CANDIDATES)
     assert len({tuner.schedule_key(s) for s in c}) == n
     for s in c:
         assert set(s) == set(DEFAULT_SCHEDULE)
