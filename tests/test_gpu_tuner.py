@@ -150,8 +150,8 @@ def test_autotuner_sweep_and_cache(ctx, tmp_path):
 def test_tuning_study_end_to_end(ctx):
     pytest.importorskip("torch")
     train, test = tuner.tuning_suite(n_train=4, n_test=2, seed=31)
-    cands = tuner.candidate_space({"warps": (4, 8), "min_blocks": (4,), "prefetch": (0, 1), "cut_adds": (0, 1)},
-                                  {"ctas_per_sm": (0,), "range_steps": (64,)})
+    cands = tuner.candidate_space({"warps": (4, 8), "min_blocks": (4,), "prefetch": (0, 1), "cut_adds": (0, 1, 2)},
+                                  {"ctas_per_sm": (0,), "range_steps": (64,)}, seq={})
     rep = tuner.study(ctx, train, test[:1], sizes=(1 << 21, 1 << 23), candidates=cands, sample_frac=0.5,
                       reps=2, steps=300)
     assert rep["loss_last"] < rep["loss_first"]
