@@ -56,19 +56,20 @@ LAUNCH_AXES = {"ctas_per_sm": (0, 2)}
 # The thread-sequential form (layout 1): its register-resident chunk needs
 # the full register file (min_blocks 1; at min_blocks 2 the 2,000-op regex
 # DAG spills and runs 2x slower), and prefetch / range_steps do not apply.
-# Its axes: 4- or 8-word register chunks, and shifts as funnel shifts (ALU
-# pipe) or as integer multiply-adds (multiply pipe).
-SEQ_AXES = {"layout": (1,), "warps": (4, 8), "min_blocks": (1,), "prefetch": (0,), "cut_adds": (0,),
-            "ctas_per_sm": (0,), "chunk_words": (4, 8), "shift_mul": (0, 1)}
-# The TMA form (layout 2): 4-word rows for 8 warps per CTA (2 or 3 stages,
-# funnel or multiply shifts), 4-word rows for 4 warps (two CTAs per SM);
-# 8-word rows leave room for only 4 warps per SM and measured 1.7x slower on
-# the regex DAG, so they are out.
+# Its axes: CTA size (2 to 16 warps: 16 warps cap registers at 128 per
+# thread) and 4- or 8-word register chunks.  Shifts as integer multiply-adds
+# (shift_mul) measured slower on the regex DAG (0.228 vs 0.211 ms) and on
+# batches, so the space keeps the funnel shifts.
+SEQ_AXES = {"layout": (1,), "warps": (2, 4, 8, 16), "min_blocks": (1,), "prefetch": (0,), "cut_adds": (0,),
+            "ctas_per_sm": (0,), "chunk_words": (4, 8)}
+# The TMA form (layout 2): 4-word rows for 8 warps per CTA (2 or 3 stages)
+# and for 4 warps (two CTAs per SM; 2 or 3 stages); 8-word rows leave room
+# for only 4 warps per SM and measured 1.7x slower on the regex DAG, so they
+# are out.
 TMA_CANDIDATES = [{"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1, "prefetch": 0, "stages": 2},
                   {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1, "prefetch": 0, "stages": 3},
                   {"layout": 2, "chunk_words": 4, "warps": 4, "min_blocks": 1, "prefetch": 0, "stages": 2},
-                  {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1, "prefetch": 0, "stages": 2,
-                   "shift_mul": 1}]
+                  {"layout": 2, "chunk_words": 4, "warps": 4, "min_blocks": 1, "prefetch": 0, "stages": 3}]
 # The carry-scheme axis: every addition run by the plain single-pass
 # carry scan (decoupled look-back) on materialized operands, the rest of
 # the DAG in generated kernels of each form (cut_adds 2), against the
