@@ -369,17 +369,22 @@ class CostModel:
 
     @classmethod
     def load_default(cls, ctx, path: str | None = None):
-        """The shipped model, or None when it has not been trained."""
+        """The shipped model, or None when it has not been trained for the
+        current feature encoding."""
         path = path or DEFAULT_MODEL_PATH
         if not os.path.exists(path):
             return None
+        with np.load(path) as z:
+            if int(z["in_dim"][0]) != N_FEATURES:
+                return None
         m = cls(ctx, N_FEATURES)
         m.load(path)
         return m
 
     def load(self, path: str):
         z = np.load(path)
-        assert int(z["in_dim"][0]) == self.in_dim
+        if int(z["in_dim"][0]) != self.in_dim:
+            raise ValueError(f"{path}: a model over {int(z['in_dim'][0])} features, not {self.in_dim}")
         self.set_params(z["params"])
         self.mu, self.sd = z["mu"], z["sd"]
         self.y_mu, self.y_sd = float(z["y"][0]), float(z["y"][1])
