@@ -194,6 +194,27 @@ def test_add_rejects_bitlength_outside_the_words(ctx):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("in_place", [False, True])
+def test_add_carry_ripples_across_many_tiles(ctx, in_place):
+    """A carry generated once and propagated over ~30 tiles (a = 0, b = all
+    ones), between random words: tiles inside the run cannot resolve their
+    carry in locally and take it by look-back."""
+    n = 50 * 4096 + 13
+    rng = np.random.default_rng(31)
+    a, b = rand_words(rng, n), rand_words(rng, n)
+    a[1000], b[1000] = np.uint64(2**64 - 1), np.uint64(1)
+    a[1001:120001] = np.uint64(0)
+    b[1001:120001] = np.uint64(2**64 - 1)
+    a[150000:150100] = ~b[150000:150100]   # a short propagate run with whatever comes in
+    da, db = dev(a), dev(b)
+    dd = da if in_place else torch.empty(n, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    ctx.op("add", dd.data_ptr(), da.data_ptr(), db.data_ptr(), n, 64 * n - 5)
+    ctx.sync()
+    assert np.array_equal(host(dd), cwords.add(a, b, 64 * n - 5))
+
+
+@pytest.mark.gpu
 def test_add_lookback_timeout_is_reported(ctx):
     """A look-back wait that runs out (its predecessor tile never publishes,
     through the test hook) ends with an error the host reads; the context
@@ -202,7 +223,10 @@ def test_add_lookback_timeout_is_reported(ctx):
     lib = _lib.load()
     n = 4 * 4096
     rng = np.random.default_rng(29)
-    a, b = rand_words(rng, n), rand_words(rng, n)
+    # b = ~a: every word propagates, so no tile can take its carry in from
+    # the words before it and every tile past the first must look back
+    a = rand_words(rng, n)
+    b = ~a
     da, db, dd = dev(a), dev(b), torch.empty(n, dtype=torch.int64, device="cuda")
     torch.cuda.synchronize()
     lib.bsz_debug_add_lookback_hook(1, 1000)

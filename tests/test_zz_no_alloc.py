@@ -95,3 +95,29 @@ def test_noalloc_add_rejects_streams_beyond_its_scratch():
     rc = lib.bsz_add_noalloc(dummy, dummy, dummy, too_long, 64 * too_long, None)
     assert rc != 0
     assert "exceeds the maximum" in _lib.last_error()
+
+
+@pytest.mark.gpu
+def test_noalloc_add_reports_a_lookback_timeout():
+    """A look-back wait that runs out (a tile that never publishes its
+    status, through the library's test hook; b = ~a so every tile must look
+    back) makes the call return nonzero with the timeout message; the next
+    call is exact."""
+    lib = _lib.load()
+    n = 4 * 4096
+    rng = np.random.default_rng(41)
+    a = rng.integers(0, 2**64, size=n, dtype=np.uint64)
+    b = ~a
+    da, db = _dev(a), _dev(b)
+    out = torch.empty(n, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    lib.bsz_debug_add_lookback_hook(1, 1000)
+    try:
+        rc = lib.bsz_add_noalloc(out.data_ptr(), da.data_ptr(), db.data_ptr(), n, 64 * n, None)
+        assert rc != 0
+        assert "timed out" in _lib.last_error()
+    finally:
+        lib.bsz_debug_add_lookback_hook(-1, 0)
+    assert lib.bsz_add_noalloc(out.data_ptr(), da.data_ptr(), db.data_ptr(), n, 64 * n, None) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy().view(np.uint64), cwords.add(a, b, 64 * n))
