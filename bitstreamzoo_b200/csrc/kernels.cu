@@ -178,27 +178,40 @@ k_shr(uint64_t* __restrict__ d, const uint64_t* __restrict__ a, int64_t ws, int 
 }
 
 // ---- add: single-pass carry scan ----------------------------------------
-// The tile of the decoupled look-back is one WARP's: kAddSteps consecutive
-// 128-word steps (kAddTile words).  In a step, lane l owns the 4-word block
-// at 4l: one 32-byte sector, a 256-bit load or store per lane, so every warp
-// access is one contiguous kilobyte.  A CTA draws one ticket for kAddWarps
-// consecutive tiles; after that its warps are independent: each publishes its
-// aggregate as soon as its loads have landed and resolves its carry in by
-// look-back with no CTA barrier, so a warp waiting on its predecessor holds
-// up nobody else on the SM.
+// The tile is one WARP's: kAddSteps consecutive 32-word steps (kAddTile
+// words; lane = word in a step, so every load and store is a coalesced
+// 256-byte warp access, kAddSteps of each in flight per operand).  A CTA
+// draws one ticket for kAddWarps consecutive tiles (same-address atomics
+// serialize, so one per warp would cost ~5 ns x 2^17 tiles); after that its
+// warps are independent.
 //
-// Carry resolution inside a step: per block, generate g (the block sum with
-// no carry in overflowed) and propagate p (a ^ b is all ones over the block:
-// then, and only then, the carry out equals the carry in).  The carries into
-// the 32 blocks are the internal carries of the 32-bit addition
-// (G|P) + G + cin: carry into lane i = bit i of ((G|P)+G+cin) ^ P, carry out
-// = bit 32.  Across steps the (g, p) pairs compose; across tiles the status
-// word is flag | g | p<<1, with bounded spins.  dst may be a or b exactly
-// (each word is read before it is written, by the one thread that writes
-// it); partial overlaps are not allowed.
+// Carry into a tile.  The word just before the tile decides it whenever that
+// word does not propagate (a ^ b != ~0: then its carry out is its own
+// overflow, whatever comes in), so almost every tile reads that one word and
+// needs nothing from any other tile.  Only a tile whose preceding word
+// propagates resolves its carry in by decoupled look-back: it publishes its
+// aggregate, walks back over its predecessors' status words (flag | g |
+// p<<1; bounded spins, a wait that runs out sets kErrLookbackTimeout) and
+// publishes its inclusive carry out.  Every tile publishes its inclusive
+// carry out as soon as it is known, so a look-back stops at the first tile
+// before the propagate run.  The ticket order makes every predecessor a tile
+// that has started, so a wait always ends.
+//
+// dst may be a or b exactly (each word is read before it is written, by the
+// one thread that writes it); then the word before a tile may already hold
+// its sum, so that call resolves every carry in by look-back (in_place).
+// Partial overlaps are not allowed.
+//
+// Carry resolution inside a step: per word, generate g (the sum with no
+// carry in overflowed) and propagate p (a ^ b is all ones: then, and only
+// then, the carry out equals the carry in).  The carries into the 32 lanes
+// are the internal carries of the 32-bit addition (G|P) + G + cin: carry
+// into lane i = bit i of ((G|P)+G+cin) ^ P, carry out = bit 32.  Across
+// steps the (g, p) pairs compose.
 constexpr int kAddWarps = 8;   // warps per CTA (independent tiles)
-constexpr int kAddSteps = 4;
-constexpr int64_t kAddTile = kAddSteps * 128;
+constexpr int kAddSteps = 16;
+constexpr int kAddMinBlocks = 1;
+constexpr int64_t kAddTile = kAddSteps * 32;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kFlagMask = 3u << 30;
@@ -217,109 +230,80 @@ __device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) {
   *reinterpret_cast<volatile uint32_t*>(p) = v;
 }
 
-// 4 words at word index w (w % 4 == 0): one 256-bit load when the block is
-// whole and the pointer 32-byte aligned, else word by word (zero past n).
-// Plain (coherent) loads: dst may alias the operand.
-template <bool VEC>
-__device__ __forceinline__ void load4(const uint64_t* p, int64_t w, int64_t n, uint64_t r[4]) {
-  if (VEC && w + 3 < n) {
-    asm volatile("ld.global.v4.u64 {%0,%1,%2,%3}, [%4];"
-                 : "=l"(r[0]), "=l"(r[1]), "=l"(r[2]), "=l"(r[3])
-                 : "l"(p + w));
-  } else {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) r[i] = (w + i < n) ? p[w + i] : 0;
+// Decoupled look-back for `tile` (> 0) with aggregate (tg, tp): returns the
+// carry into the tile and publishes the tile's inclusive carry out.
+__device__ __forceinline__ uint32_t add_lookback(uint32_t* status, int64_t tile, uint32_t tg, uint32_t tp,
+                                                 uint32_t* err, int spin_limit) {
+  st_volatile(&status[tile], kFlagAgg | tg | (tp << 1));
+  uint32_t ag = 0, ap = 1, cin = 0;
+  int64_t j = tile - 1;
+  int spins = 0;
+  while (true) {
+    const uint32_t v = ld_volatile(&status[j]);
+    const uint32_t f = v & kFlagMask;
+    if (f == 0) {
+      if (++spins > spin_limit) {
+        atomicOr(err, kErrLookbackTimeout);
+        cin = 0;
+        break;
+      }
+      __nanosleep(32);
+      continue;
+    }
+    if (f == kFlagInc) {
+      cin = ag | (ap & (v & 1u));
+      break;
+    }
+    const uint32_t g = v & 1u, p = (v >> 1) & 1u;
+    ag = ag | (ap & g);
+    ap &= p;
+    if (!ap) {   // the carry out of the walked range no longer depends on earlier tiles
+      cin = ag;
+      break;
+    }
+    --j;
+    spins = 0;
   }
+  st_volatile(&status[tile], kFlagInc | (tg | (tp & cin)));
+  return cin;
 }
 
-template <bool VEC>
-__device__ __forceinline__ void store4(uint64_t* p, int64_t w, int64_t n, const uint64_t r[4]) {
-  if (VEC && w + 3 < n) {
-    asm volatile("st.global.v4.u64 [%0], {%1,%2,%3,%4};" ::"l"(p + w), "l"(r[0]), "l"(r[1]), "l"(r[2]),
-                 "l"(r[3])
-                 : "memory");
-  } else {
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-      if (w + i < n) p[w + i] = r[i];
-  }
-}
-
-#define BSZ_LO(x) static_cast<uint32_t>(x)
-#define BSZ_HI(x) static_cast<uint32_t>((x) >> 32)
-
-// s = a + b over a 256-bit block (no carry in); returns the carry out.
-__device__ __forceinline__ uint32_t add4(uint64_t s[4], const uint64_t a[4], const uint64_t b[4]) {
-  uint32_t r[8], c;
-  asm("add.cc.u32 %0, %9, %17;\n\t"
-      "addc.cc.u32 %1, %10, %18;\n\t"
-      "addc.cc.u32 %2, %11, %19;\n\t"
-      "addc.cc.u32 %3, %12, %20;\n\t"
-      "addc.cc.u32 %4, %13, %21;\n\t"
-      "addc.cc.u32 %5, %14, %22;\n\t"
-      "addc.cc.u32 %6, %15, %23;\n\t"
-      "addc.cc.u32 %7, %16, %24;\n\t"
-      "addc.u32 %8, 0, 0;"
-      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5]), "=&r"(r[6]),
-        "=&r"(r[7]), "=&r"(c)
-      : "r"(BSZ_LO(a[0])), "r"(BSZ_HI(a[0])), "r"(BSZ_LO(a[1])), "r"(BSZ_HI(a[1])), "r"(BSZ_LO(a[2])),
-        "r"(BSZ_HI(a[2])), "r"(BSZ_LO(a[3])), "r"(BSZ_HI(a[3])), "r"(BSZ_LO(b[0])), "r"(BSZ_HI(b[0])),
-        "r"(BSZ_LO(b[1])), "r"(BSZ_HI(b[1])), "r"(BSZ_LO(b[2])), "r"(BSZ_HI(b[2])), "r"(BSZ_LO(b[3])),
-        "r"(BSZ_HI(b[3])));
-#pragma unroll
-  for (int i = 0; i < 4; ++i) s[i] = (static_cast<uint64_t>(r[2 * i + 1]) << 32) | r[2 * i];
-  return c;
-}
-
-// s += c (c in {0, 1}) over a 256-bit block.
-__device__ __forceinline__ void inc4(uint64_t s[4], uint32_t c) {
-  uint32_t r[8];
-  asm("add.cc.u32 %0, %8, %16;\n\t"
-      "addc.cc.u32 %1, %9, 0;\n\t"
-      "addc.cc.u32 %2, %10, 0;\n\t"
-      "addc.cc.u32 %3, %11, 0;\n\t"
-      "addc.cc.u32 %4, %12, 0;\n\t"
-      "addc.cc.u32 %5, %13, 0;\n\t"
-      "addc.cc.u32 %6, %14, 0;\n\t"
-      "addc.u32 %7, %15, 0;"
-      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5]), "=&r"(r[6]),
-        "=&r"(r[7])
-      : "r"(BSZ_LO(s[0])), "r"(BSZ_HI(s[0])), "r"(BSZ_LO(s[1])), "r"(BSZ_HI(s[1])), "r"(BSZ_LO(s[2])),
-        "r"(BSZ_HI(s[2])), "r"(BSZ_LO(s[3])), "r"(BSZ_HI(s[3])), "r"(c));
-#pragma unroll
-  for (int i = 0; i < 4; ++i) s[i] = (static_cast<uint64_t>(r[2 * i + 1]) << 32) | r[2 * i];
-}
-
-template <bool VEC>
-__global__ void __launch_bounds__(kAddWarps * 32)
+__global__ void __launch_bounds__(kAddWarps * 32, kAddMinBlocks)
 k_add(uint64_t* d, const uint64_t* a, const uint64_t* b, int64_t n, uint64_t last_mask,
-      uint32_t* __restrict__ state, uint32_t* __restrict__ err, int64_t silent_tile, int spin_limit) {
-  // one ticket per CTA (same-address atomics serialize: one per warp would
-  // cost ~5 ns x 2^17 tiles); its warps take the CTA's kAddWarps tiles
+      uint32_t* __restrict__ state, uint32_t* __restrict__ err, int in_place, int64_t silent_tile,
+      int spin_limit) {
   __shared__ uint32_t s_ticket;
   if (threadIdx.x == 0) s_ticket = atomicAdd(&state[0], 1u);
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int64_t tile = static_cast<int64_t>(s_ticket) * kAddWarps + (threadIdx.x >> 5);
-  const int64_t wbase = tile * kAddTile + 4 * lane;
-  if (tile * kAddTile >= n) return;   // a whole warp past the end (grid rounding)
-  uint64_t sum[kAddSteps][4];
+  const int64_t base = tile * kAddTile;
+  if (base >= n) return;   // a whole warp past the end (grid rounding)
+  // the word before the tile (not in place: nobody writes it during the call)
+  uint64_t ha = 0, hb = 0;
+  if (lane == 0 && tile > 0 && !in_place) {
+    ha = a[base - 1];
+    hb = b[base - 1];
+  }
+  uint64_t x[kAddSteps], y[kAddSteps];
+#pragma unroll
+  for (int j = 0; j < kAddSteps; ++j) {
+    const int64_t w = base + lane + j * 32;
+    x[j] = 0;
+    y[j] = 0;
+    if (w < n) {
+      x[j] = a[w];
+      y[j] = b[w];
+    }
+  }
   uint32_t G[kAddSteps], P[kAddSteps];
-  {
-    uint64_t x[kAddSteps][4], y[kAddSteps][4];
 #pragma unroll
-    for (int j = 0; j < kAddSteps; ++j) {
-      load4<VEC>(a, wbase + j * 128, n, x[j]);
-      load4<VEC>(b, wbase + j * 128, n, y[j]);
-    }
-#pragma unroll
-    for (int j = 0; j < kAddSteps; ++j) {
-      const uint32_t g = add4(sum[j], x[j], y[j]);
-      const uint64_t q = (x[j][0] ^ y[j][0]) & (x[j][1] ^ y[j][1]) & (x[j][2] ^ y[j][2]) & (x[j][3] ^ y[j][3]);
-      G[j] = __ballot_sync(0xffffffffu, g != 0);
-      // words past n are zero in both operands, so their blocks never propagate
-      P[j] = __ballot_sync(0xffffffffu, q == ~uint64_t(0));
-    }
+  for (int j = 0; j < kAddSteps; ++j) {
+    const uint64_t sj = x[j] + y[j];
+    G[j] = __ballot_sync(0xffffffffu, sj < x[j]);
+    // words past n are zero in both operands, so they never propagate
+    P[j] = __ballot_sync(0xffffffffu, (x[j] ^ y[j]) == ~uint64_t(0));
+    x[j] = sj;
   }
   // the tile's aggregate over its steps (in word order)
   uint32_t tg = 0, tp = 1;
@@ -336,40 +320,11 @@ k_add(uint64_t* d, const uint64_t* a, const uint64_t* b, int64_t n, uint64_t las
     uint32_t* status = state + 1;
     if (tile == 0) {
       st_volatile(&status[0], kFlagInc | tg);
-    } else {
-      st_volatile(&status[tile], kFlagAgg | tg | (tp << 1));
-      // walk back: (ag, ap) = composition of the tiles between j and this one
-      uint32_t ag = 0, ap = 1;
-      int64_t j = tile - 1;
-      int spins = 0;
-      while (true) {
-        const uint32_t v = ld_volatile(&status[j]);
-        const uint32_t f = v & kFlagMask;
-        if (f == 0) {
-          if (++spins > spin_limit) {
-            atomicOr(err, kErrLookbackTimeout);
-            cin = 0;
-            break;
-          }
-          __nanosleep(32);
-          continue;
-        }
-        if (f == kFlagInc) {
-          cin = ag | (ap & (v & 1u));
-          break;
-        }
-        const uint32_t g = v & 1u, p = (v >> 1) & 1u;
-        ag = ag | (ap & g);
-        ap &= p;
-        if (!ap) {   // the carry out of the walked range no longer depends on earlier tiles
-          cin = ag;
-          break;
-        }
-        --j;
-        spins = 0;
-      }
-      __threadfence();
+    } else if (!in_place && (ha ^ hb) != ~uint64_t(0)) {
+      cin = (ha + hb) < ha;   // the preceding word's own overflow is its carry out
       st_volatile(&status[tile], kFlagInc | (tg | (tp & cin)));
+    } else {
+      cin = add_lookback(status, tile, tg, tp, err, spin_limit);
     }
   }
   uint32_t c = __shfl_sync(0xffffffffu, cin, 0);
@@ -378,21 +333,15 @@ k_add(uint64_t* d, const uint64_t* a, const uint64_t* b, int64_t n, uint64_t las
     const uint64_t z = static_cast<uint64_t>(G[j] | P[j]) + G[j] + c;
     const uint32_t carries = static_cast<uint32_t>(z) ^ P[j];
     c = static_cast<uint32_t>(z >> 32);
-    const int64_t w = wbase + j * 128;
+    const int64_t w = base + lane + j * 32;
     if (w < n) {
-      inc4(sum[j], (carries >> lane) & 1u);
-      if (w + 3 >= n - 1) {   // this block holds the last word
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-          if (w + i == n - 1) sum[j][i] &= last_mask;
-      }
-      store4<VEC>(d, w, n, sum[j]);
+      uint64_t r = x[j] + ((carries >> lane) & 1u);
+      if (w == n - 1) r &= last_mask;
+      d[w] = r;
     }
   }
 }
 
-#undef BSZ_LO
-#undef BSZ_HI
 
 // ---- reductions ------------------------------------------------------------
 __device__ __forceinline__ uint64_t warp_sum(uint64_t v) {
@@ -495,19 +444,16 @@ void launch_shr(Device& dev, uint64_t* d, const uint64_t* a, int64_t k, int64_t 
 
 int64_t add_state_words(int64_t n) { return 1 + (n + kAddTile - 1) / kAddTile; }
 
-static bool aligned32(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 31) == 0; }
-
 static void launch_add_kernel(cudaStream_t stream, uint64_t* d, const uint64_t* a, const uint64_t* b,
                               int64_t n, uint64_t last_mask, uint32_t* state, uint32_t* err) {
   const int64_t tiles = (n + kAddTile - 1) / kAddTile;
   if (tiles > 0x7fffffff) throw std::invalid_argument("launch_add: stream too long");
-  const bool vec = aligned32(d) && aligned32(a) && aligned32(b);
-  auto k = vec ? k_add<true> : k_add<false>;
-  // one warp per tile (each warp draws its own ticket)
+  const int in_place = (d == a || d == b) ? 1 : 0;
+  // one warp per tile, one ticket per CTA of kAddWarps tiles
   const int64_t blocks = (tiles + kAddWarps - 1) / kAddWarps;
   if (blocks > 0x7fffffff) throw std::invalid_argument("launch_add: stream too long");
-  k<<<static_cast<unsigned>(blocks), kAddWarps * 32, 0, stream>>>(d, a, b, n, last_mask, state, err,
-                                                                  g_add_silent_tile, g_add_spin_limit);
+  k_add<<<static_cast<unsigned>(blocks), kAddWarps * 32, 0, stream>>>(d, a, b, n, last_mask, state, err, in_place,
+                                                                      g_add_silent_tile, g_add_spin_limit);
   check_launch();
 }
 
