@@ -241,6 +241,18 @@ class Run:
         self.stats = st.as_dict()
         return self.stats
 
+    def launch(self):
+        """Enqueue the run's device work and return without waiting
+        (``bsz_execute_async``); :meth:`wait` (or reading any result)
+        finishes it."""
+        _lib.check(self.lib.bsz_execute_async(self.h))
+
+    def wait(self) -> dict:
+        st = Stats()
+        _lib.check(self.lib.bsz_run_wait(self.h, ctypes.byref(st)))
+        self.stats = st.as_dict()
+        return self.stats
+
     def stream(self, name: str, index: int = -1) -> np.ndarray:
         out = np.empty(self.nw, dtype=np.uint64)
         _lib.check(self.lib.bsz_get_stream(self.h, name.encode(), index, out.ctypes.data, self.nw))

@@ -68,6 +68,8 @@ SIGNATURES = {
     "bsz_bind_broadcast": (ctypes.c_int, [c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint8),
                                           ctypes.c_int64]),
     "bsz_execute": (ctypes.c_int, [c_void_p, ctypes.POINTER(Stats)]),
+    "bsz_execute_async": (ctypes.c_int, [c_void_p]),
+    "bsz_run_wait": (ctypes.c_int, [c_void_p, ctypes.POINTER(Stats)]),
     "bsz_get_stream": (ctypes.c_int, [c_void_p, ctypes.c_char_p, ctypes.c_int64, c_void_p,
                                       ctypes.c_uint64]),
     "bsz_get_stream_device": (ctypes.c_int, [c_void_p, ctypes.c_char_p, ctypes.c_int64,

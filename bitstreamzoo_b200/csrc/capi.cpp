@@ -46,9 +46,14 @@ struct bsz_run {
   int mode;
   std::unique_ptr<bsz::Executor> ex;
   std::vector<std::pair<int, int64_t>> params;
-  bool done = false;
+  bool launched = false;   // bsz_execute_async enqueued its work
+  bool done = false;       // finished: results readable
+  int64_t l0 = 0;          // the device's launch count before this run
+  cudaEvent_t ev[2] = {nullptr, nullptr};   // device-time window of this run
   ~bsz_run() {
     ex.reset();
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
     prog_unref(prog);
   }
 };
@@ -280,39 +285,69 @@ int bsz_bind_broadcast(bsz_run* run, const char* name, const uint8_t* ones, int6
   });
 }
 
+static void launch_run(bsz_run* run) {
+  if (run->done || run->launched) throw bsz::RuntimeError("bsz_execute: run already executed");
+  bsz::Device& dev = *run->prog->ctx->dev;
+  bsz::Executor& ex = executor(run);
+  for (cudaEvent_t& e : run->ev)
+    if (!e) BSZ_CUDA(cudaEventCreate(&e));
+  run->l0 = dev.n_launches;
+  BSZ_CUDA(cudaEventRecord(run->ev[0], dev.stream()));
+  ex.run(false);
+  BSZ_CUDA(cudaEventRecord(run->ev[1], dev.stream()));
+  run->launched = true;
+}
+
+static void finish_run(bsz_run* run, bsz_stats* stats) {
+  if (!run->launched) throw bsz::RuntimeError("bsz_run_wait: run not launched");
+  bsz::Device& dev = *run->prog->ctx->dev;
+  bsz::Executor& ex = executor(run);
+  if (!run->done) {
+    ex.finish();
+    BSZ_CUDA(cudaEventSynchronize(run->ev[1]));
+    run->done = true;
+  }
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, run->ev[0], run->ev[1]);
+    stats->op_count = ex.op_count;
+    stats->n_kernel_launches = dev.n_launches - run->l0;
+    stats->n_mallocs = dev.n_mallocs;
+    stats->n_segments = ex.n_segments;
+    stats->n_syncs = ex.n_syncs;
+    stats->peak_bytes = dev.bytes_peak;
+    stats->max_live = ex.max_live_buffers;
+    stats->kernel_ms = ms;
+    stats->compile_ms = ex.compile_ms;
+    stats->n_fused_launches = ex.fused_launches();
+    stats->n_fused_fallbacks = ex.fused_fallbacks();
+    stats->n_vm_launches = ex.vm_launches;
+    stats->walk_replayed = ex.walk_replayed ? 1 : 0;
+  }
+}
+
+// Results of a launched run are readable once it has finished.
+static void ensure_finished(bsz_run* run) {
+  if (run->launched && !run->done) finish_run(run, nullptr);
+}
+
 int bsz_execute(bsz_run* run, bsz_stats* stats) {
   return guard([&] {
-    if (run->done) throw bsz::RuntimeError("bsz_execute: run already executed");
-    bsz::Device& dev = *run->prog->ctx->dev;
-    bsz::Executor& ex = executor(run);
-    const int64_t l0 = dev.n_launches;
-    cudaEvent_t e0 = dev.exec_event(0), e1 = dev.exec_event(1);
-    BSZ_CUDA(cudaEventRecord(e0, dev.stream()));
-    ex.run();
-    BSZ_CUDA(cudaEventRecord(e1, dev.stream()));
-    BSZ_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    run->done = true;
-    if (stats) {
-      stats->op_count = ex.op_count;
-      stats->n_kernel_launches = dev.n_launches - l0;
-      stats->n_mallocs = dev.n_mallocs;
-      stats->n_segments = ex.n_segments;
-      stats->n_syncs = ex.n_syncs;
-      stats->peak_bytes = dev.bytes_peak;
-      stats->max_live = ex.max_live_buffers;
-      stats->kernel_ms = ms;
-      stats->compile_ms = ex.compile_ms;
-      stats->n_fused_launches = ex.fused_launches();
-      stats->n_fused_fallbacks = ex.fused_fallbacks();
-      stats->n_vm_launches = ex.vm_launches;
-      stats->walk_replayed = ex.walk_replayed ? 1 : 0;
-    }
+    launch_run(run);
+    finish_run(run, stats);
   });
 }
 
+int bsz_execute_async(bsz_run* run) {
+  return guard([&] { launch_run(run); });
+}
+
+int bsz_run_wait(bsz_run* run, bsz_stats* stats) {
+  return guard([&] { finish_run(run, stats); });
+}
+
 static bsz::BufRef find_stream(bsz_run* run, const char* name, int64_t index) {
+  ensure_finished(run);
   bsz::Executor& ex = executor(run);
   int id = name_id(run, name);
   bsz::BufRef b = index < 0 ? ex.stream_value(id) : ex.array_value(id, index);
@@ -343,6 +378,7 @@ int bsz_get_stream_device(bsz_run* run, const char* name, int64_t index, const u
 
 int bsz_get_int(bsz_run* run, const char* name, int64_t* value) {
   return guard([&] {
+    ensure_finished(run);
     if (!executor(run).int_value(name_id(run, name), value))
       throw std::invalid_argument(std::string("no such int: ") + name);
   });
@@ -351,6 +387,7 @@ int bsz_get_int(bsz_run* run, const char* name, int64_t* value) {
 int64_t bsz_array_indices(bsz_run* run, const char* name, int64_t* indices, int64_t cap) {
   int64_t count = -1;
   guard([&] {
+    ensure_finished(run);
     int id = name_id(run, name);
     if (!executor(run).has_array(id)) return;
     auto idx = executor(run).array_indices(id);

@@ -609,7 +609,7 @@ bool has_control_flow(const std::vector<Stmt>& v) {
 }
 }  // namespace
 
-void Executor::run() {
+void Executor::run(bool finish_now) {
   // Programs with if/while on short streams: the whole program, branches
   // included, runs as one launch of the device interpreter (no host round
   // trip per condition) when it qualifies.
@@ -632,7 +632,6 @@ void Executor::run() {
     if (straight && n_flushes_ == f0) save_walk(key, n0);
   }
   flush(&live_->end, nullptr);
-  resolve_slots();
   publish_op_mix();
   // Outputs bound to constants get a buffer so the caller can read them.
   auto materialize = [&](int& node) {
@@ -649,6 +648,12 @@ void Executor::run() {
     if (arrs_[id])
       for (auto& kv : arrs_[id]->elems) materialize(kv.second);
   }
+  if (finish_now) finish();
+}
+
+void Executor::finish() {
+  if (fused_) fused_->resolve();
+  resolve_slots();
   if (uint32_t err = dev_.take_error()) throw RuntimeError(describe_device_error(err));
 }
 
@@ -661,6 +666,9 @@ void Executor::flush(const Bits* live, int* extra) {
                        "index or shift amount)");
   using clk = std::chrono::steady_clock;
   auto ms_since = [](clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); };
+  // a fused segment still pending (its speculation unchecked) must be exact
+  // before anything runs after it
+  if (fused_) fused_->resolve();
   auto t0 = clk::now();
   ++n_flushes_;
   const int n_nodes = static_cast<int>(nodes_.size());
@@ -986,6 +994,7 @@ void Executor::ensure_slots(int64_t need) {
 
 void Executor::resolve_slots() {
   if (!pending_pops_.empty()) flush(nullptr, nullptr);
+  if (fused_) fused_->resolve();
   if (resolved_upto_ < n_slots_) {
     int64_t from = resolved_upto_ - slot_base_;
     int64_t cnt = n_slots_ - resolved_upto_;

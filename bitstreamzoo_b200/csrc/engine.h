@@ -101,7 +101,13 @@ class Executor {
   void bind_input_array(int name, int64_t idx, BufRef buf, uint8_t tail, bool clean);
   void bind_broadcast(int name, const std::vector<uint8_t>& ones);   // element i: 1 = -1
 
-  void run();
+  // Walks the program and enqueues its device work.  With finish = false it
+  // returns without waiting for the device (no host read-back at the end):
+  // call finish() before reading results.
+  void run(bool finish = true);
+  // Waits for the enqueued work, re-runs any fused part whose speculation
+  // was unproven, reads the popcount slots and checks the device error word.
+  void finish();
 
   // Results (valid after run()).
   bool has_stream(int name) const;

@@ -137,36 +137,6 @@ bool is_const(NOp op) { return op == NOp::Zero || op == NOp::OnesMask || op == N
 
 }  // namespace
 
-struct FusedBackend::Impl {
-  Device& dev;
-  ExecOptions opt;
-  BufRef fail_buf;   // from the device's buffer cache: no cudaMalloc/cudaFree per run
-  unsigned int* d_fail = nullptr;
-  Impl(Device& d, const ExecOptions& o) : dev(d), opt(o) {
-    fail_buf = dev.alloc_stream(32);
-    d_fail = reinterpret_cast<unsigned int*>(fail_buf->p);
-  }
-};
-
-FusedBackend::FusedBackend(Device& dev, const ExecOptions& opt)
-    : impl_(std::make_unique<Impl>(dev, opt)) {}
-FusedBackend::~FusedBackend() = default;
-
-void FusedBackend::set_schedule(const Schedule& s) {
-  Schedule c = s;
-  c.warps = std::max(1, std::min(c.warps, 16));
-  c.range_steps = std::max(1, c.range_steps);
-  c.ctas_per_sm = std::max(-1, c.ctas_per_sm);
-  c.min_blocks = std::max(1, std::min(c.min_blocks, 32));
-  c.layout = std::max(0, std::min(c.layout, 2));
-  c.cut_adds = std::max(0, std::min(c.cut_adds, 2));
-  c.chunk_words = c.chunk_words == 8 ? 8 : 4;
-  c.stages = c.stages == 3 ? 3 : 2;
-  c.unroll = c.unroll ? 1 : 0;
-  c.shift_mul = c.shift_mul ? 1 : 0;
-  impl_->opt.sched = c;
-}
-
 namespace {
 
 // One kernel's worth of the segment.
@@ -1709,6 +1679,53 @@ PartKernel part_kernel(const std::vector<Node>& nodes, const Part& p, int64_t N,
 
 }  // namespace
 
+// A launched segment whose speculation flags have not been read yet: its
+// parts, a copy of every node they compute or read (with the buffers, so
+// none returns to the cache while a re-run may need it) and where its
+// popcounts go.
+struct PendingSegment {
+  std::shared_ptr<const void> plan;          // keeps `parts` alive
+  const std::vector<Part>* parts = nullptr;
+  std::unordered_map<int, Node> nodes;
+  int64_t N = 0, nw = 0;
+  unsigned long long* d_slots = nullptr;
+};
+
+struct FusedBackend::Impl {
+  Device& dev;
+  ExecOptions opt;
+  BufRef fail_buf;   // from the device's buffer cache: no cudaMalloc/cudaFree per run
+  unsigned int* d_fail = nullptr;   // one flag per part of the launched segment
+  int64_t fail_cap = 0;
+  std::unique_ptr<PendingSegment> pending;
+  Impl(Device& d, const ExecOptions& o) : dev(d), opt(o) { ensure_flags(64); }
+  void ensure_flags(int64_t n) {
+    if (n <= fail_cap) return;
+    fail_cap = std::max<int64_t>(n, 2 * fail_cap);
+    fail_buf = dev.alloc_stream((fail_cap + 1) / 2);
+    d_fail = reinterpret_cast<unsigned int*>(fail_buf->p);
+  }
+};
+
+FusedBackend::FusedBackend(Device& dev, const ExecOptions& opt)
+    : impl_(std::make_unique<Impl>(dev, opt)) {}
+FusedBackend::~FusedBackend() = default;
+
+void FusedBackend::set_schedule(const Schedule& s) {
+  Schedule c = s;
+  c.warps = std::max(1, std::min(c.warps, 16));
+  c.range_steps = std::max(1, c.range_steps);
+  c.ctas_per_sm = std::max(-1, c.ctas_per_sm);
+  c.min_blocks = std::max(1, std::min(c.min_blocks, 32));
+  c.layout = std::max(0, std::min(c.layout, 2));
+  c.cut_adds = std::max(0, std::min(c.cut_adds, 2));
+  c.chunk_words = c.chunk_words == 8 ? 8 : 4;
+  c.stages = c.stages == 3 ? 3 : 2;
+  c.unroll = c.unroll ? 1 : 0;
+  c.shift_mul = c.shift_mul ? 1 : 0;
+  impl_->opt.sched = c;
+}
+
 bool FusedBackend::all_compiled(const std::vector<Node>& nodes, const Segment& seg, int64_t N) {
   const Schedule& sc = impl_->opt.sched;
   {
@@ -1784,6 +1801,10 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
     plan_cache()[skey] = np;
     plan = np;
   }
+  // one speculation flag per part, read once by resolve()
+  resolve();
+  impl_->ensure_flags(static_cast<int64_t>(plan->parts.size()));
+  BSZ_CUDA(cudaMemsetAsync(impl_->d_fail, 0, 4 * plan->parts.size(), dev.stream()));
   for (size_t pi = 0; pi < plan->parts.size(); ++pi) {
     const Part& p = plan->parts[pi];
     const PartKernel& pk = plan->kernels[pi];
@@ -1864,7 +1885,7 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
       uint64_t* tail = reinterpret_cast<uint64_t*>(targs.data() + maps_bytes);
       for (int i = 0; i < ni + no; ++i) tail[i] = args[i];
       tail[ni + no + 0] = reinterpret_cast<uint64_t>(d_slots);
-      tail[ni + no + 1] = reinterpret_cast<uint64_t>(impl_->d_fail);
+      tail[ni + no + 1] = reinterpret_cast<uint64_t>(impl_->d_fail + pi);
       tail[ni + no + 2] = static_cast<uint64_t>(nw);
       tail[ni + no + 3] = static_cast<uint64_t>(range);
       tail[ni + no + 4] = mask_for_bits(N);
@@ -1897,11 +1918,10 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
       blocks = static_cast<int>((total_warps + sc.warps - 1) / sc.warps);
     }
     args[ni + no + 0] = reinterpret_cast<uint64_t>(d_slots);
-    args[ni + no + 1] = reinterpret_cast<uint64_t>(impl_->d_fail);
+    args[ni + no + 1] = reinterpret_cast<uint64_t>(impl_->d_fail + pi);
     args[ni + no + 2] = static_cast<uint64_t>(nw);
     args[ni + no + 3] = static_cast<uint64_t>(range);
     args[ni + no + 4] = mask_for_bits(N);
-    BSZ_CUDA(cudaMemsetAsync(impl_->d_fail, 0, 4, dev.stream()));
     void* kparams[] = {pk.roww > 0 ? static_cast<void*>(targs.data()) : static_cast<void*>(args.data())};
     {
       ProfScope prof(dev, "fused");
@@ -1911,63 +1931,98 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
     ++dev.n_launches;
     ++launches;
     t_prelaunch_ms += ms_since(tp);
-    auto tw = clk::now();
-    unsigned int fail = 0;
-    BSZ_CUDA(cudaMemcpyAsync(&fail, impl_->d_fail, 4, cudaMemcpyDeviceToHost, dev.stream()));
-    BSZ_CUDA(cudaStreamSynchronize(dev.stream()));
-    t_wait_ms += ms_since(tw);
     tp = clk::now();
-    if (fail) {
-      // Speculation could not be proven exact: redo this part with the plain
-      // per-op kernels (exact by construction).
-      for (auto& pp : p.pops) BSZ_CUDA(cudaMemsetAsync(d_slots + pp.second, 0, 8, dev.stream()));
-      const uint64_t lm = mask_for_bits(N);
-      std::map<int, BufRef> tmp;
-      auto ptr = [&](int n) -> const uint64_t* {
-        if (nodes[n].buf) return nodes[n].buf->p;
-        auto it = tmp.find(n);
-        if (it != tmp.end()) return it->second->p;
-        throw RuntimeError("fused fallback: operand without a buffer");
-      };
-      for (int n : p.order) {
-        const Node& x = nodes[n];
-        BufRef out = nodes[n].buf ? nodes[n].buf : dev.alloc_stream(nw);
-        uint64_t* D = out->p;
-        auto opnd = [&](int o) -> const uint64_t* {
-          const Node& y = nodes[o];
-          if (is_const(y.op)) {
-            auto it = tmp.find(o);
-            if (it == tmp.end()) {
-              BufRef b = dev.alloc_stream(nw);
-              uint64_t val = y.op == NOp::Zero ? 0 : ~uint64_t(0);
-              uint64_t last = y.op == NOp::OnesMask ? lm : val;
-              launch_fill(dev, b->p, nw, val, last);
-              it = tmp.emplace(o, b).first;
-            }
-            return it->second->p;
-          }
-          return ptr(o);
-        };
-        switch (x.op) {
-          case NOp::Not: launch_not(dev, D, opnd(x.a), nw, lm); break;
-          case NOp::And: launch_bitwise(dev, kAnd, D, opnd(x.a), opnd(x.b), nw); break;
-          case NOp::Or: launch_bitwise(dev, kOr, D, opnd(x.a), opnd(x.b), nw); break;
-          case NOp::Xor: launch_bitwise(dev, kXor, D, opnd(x.a), opnd(x.b), nw); break;
-          case NOp::AndNot: launch_bitwise(dev, kAndNot, D, opnd(x.a), opnd(x.b), nw); break;
-          case NOp::Add: launch_add(dev, D, opnd(x.a), opnd(x.b), nw, lm); break;
-          case NOp::Shl: launch_shl(dev, D, opnd(x.a), x.k, nw, lm); break;
-          case NOp::Shr: launch_shr(dev, D, opnd(x.a), x.k, nw, nodes[x.a].tail ? ~uint64_t(0) : 0); break;
-          default: throw RuntimeError("fused fallback: unexpected node");
-        }
-        if (!nodes[n].buf) tmp[n] = out;
-      }
-      for (auto& pp : p.pops) {
-        const Node& y = nodes[pp.first];
-        const uint64_t* src_ptr = y.buf ? y.buf->p : tmp.at(pp.first)->p;
-        launch_popcount(dev, src_ptr, nw, d_slots + pp.second);
-      }
-      ++fallbacks;
+  }
+  // the segment stays pending until resolve(): keep its parts and a copy of
+  // every node they compute or read, buffers included
+  auto pend = std::make_unique<PendingSegment>();
+  pend->plan = plan;
+  pend->parts = &plan->parts;
+  pend->N = N;
+  pend->nw = nw;
+  pend->d_slots = d_slots;
+  for (const Part& p : plan->parts) {
+    for (int n : p.order) pend->nodes.emplace(n, nodes[n]);
+    for (int n : p.inputs) pend->nodes.emplace(n, nodes[n]);
+    for (auto& pp : p.pops) pend->nodes.emplace(pp.first, nodes[pp.first]);
+  }
+  impl_->pending = std::move(pend);
+}
+
+bool FusedBackend::pending() const { return impl_->pending != nullptr; }
+
+namespace {
+
+// Re-runs one part with the exact per-op kernels (its popcount slots are
+// cleared first), reading and writing the buffers recorded with it.
+void rerun_part_exact(Device& dev, const Part& p, std::unordered_map<int, Node>& nodes, int64_t N, int64_t nw,
+                      unsigned long long* d_slots) {
+  for (auto& pp : p.pops) BSZ_CUDA(cudaMemsetAsync(d_slots + pp.second, 0, 8, dev.stream()));
+  const uint64_t lm = mask_for_bits(N);
+  std::map<int, BufRef> tmp;
+  auto node = [&](int n) -> Node& {
+    auto it = nodes.find(n);
+    if (it == nodes.end()) throw RuntimeError("fused re-run: a node was not recorded");
+    return it->second;
+  };
+  auto opnd = [&](int o) -> const uint64_t* {
+    const Node& y = node(o);
+    if (y.buf) return y.buf->p;
+    auto it = tmp.find(o);
+    if (it != tmp.end()) return it->second->p;
+    if (is_const(y.op)) {
+      BufRef b = dev.alloc_stream(nw);
+      const uint64_t val = y.op == NOp::Zero ? 0 : ~uint64_t(0);
+      launch_fill(dev, b->p, nw, val, y.op == NOp::OnesMask ? lm : val);
+      return tmp.emplace(o, b).first->second->p;
     }
+    throw RuntimeError("fused re-run: operand without a buffer");
+  };
+  for (int n : p.order) {
+    const Node& x = node(n);
+    BufRef out = x.buf ? x.buf : dev.alloc_stream(nw);
+    uint64_t* D = out->p;
+    switch (x.op) {
+      case NOp::Not: launch_not(dev, D, opnd(x.a), nw, lm); break;
+      case NOp::And: launch_bitwise(dev, kAnd, D, opnd(x.a), opnd(x.b), nw); break;
+      case NOp::Or: launch_bitwise(dev, kOr, D, opnd(x.a), opnd(x.b), nw); break;
+      case NOp::Xor: launch_bitwise(dev, kXor, D, opnd(x.a), opnd(x.b), nw); break;
+      case NOp::AndNot: launch_bitwise(dev, kAndNot, D, opnd(x.a), opnd(x.b), nw); break;
+      case NOp::Add: launch_add(dev, D, opnd(x.a), opnd(x.b), nw, lm); break;
+      case NOp::Shl: launch_shl(dev, D, opnd(x.a), x.k, nw, lm); break;
+      case NOp::Shr: launch_shr(dev, D, opnd(x.a), x.k, nw, node(x.a).tail ? ~uint64_t(0) : 0); break;
+      default: throw RuntimeError("fused re-run: unexpected node");
+    }
+    if (!x.buf) tmp[n] = out;
+  }
+  for (auto& pp : p.pops) launch_popcount(dev, opnd(pp.first), nw, d_slots + pp.second);
+}
+
+}  // namespace
+
+void FusedBackend::resolve() {
+  if (!impl_->pending) return;
+  std::unique_ptr<PendingSegment> pend = std::move(impl_->pending);
+  Device& dev = impl_->dev;
+  const std::vector<Part>& parts = *pend->parts;
+  using clk = std::chrono::steady_clock;
+  auto tw = clk::now();
+  std::vector<uint32_t> flags(parts.size(), 0);
+  BSZ_CUDA(cudaMemcpyAsync(flags.data(), impl_->d_fail, 4 * flags.size(), cudaMemcpyDeviceToHost, dev.stream()));
+  BSZ_CUDA(cudaStreamSynchronize(dev.stream()));
+  t_wait_ms += std::chrono::duration<double, std::milli>(clk::now() - tw).count();
+  size_t first = parts.size();
+  for (size_t i = 0; i < parts.size(); ++i)
+    if (flags[i]) {
+      first = i;
+      break;
+    }
+  // Speculation could not be proven exact in part `first`: redo it, and
+  // every later part (which may have read its outputs), with the plain
+  // per-op kernels (exact by construction).
+  for (size_t i = first; i < parts.size(); ++i) {
+    rerun_part_exact(dev, parts[i], pend->nodes, pend->N, pend->nw, pend->d_slots);
+    if (flags[i]) ++fallbacks;
   }
 }
 

@@ -18,9 +18,18 @@ class FusedBackend {
   FusedBackend(Device& dev, const ExecOptions& opt);
   ~FusedBackend();
   // Computes seg.order; materializes seg.outputs into nodes[i].buf and adds
-  // the popcounts of seg.pops into d_slots[slot].
+  // the popcounts of seg.pops into d_slots[slot].  Asynchronous: the kernels
+  // are enqueued with one speculation flag per part, and the segment stays
+  // pending (its parts, node records and buffers held) until resolve().
   void run(std::vector<Node>& nodes, const Segment& seg, int64_t N, int64_t nw,
            unsigned long long* d_slots, double* compile_ms);
+  // Waits for the pending segment, reads its parts' flags and re-runs every
+  // part from the first unproven one on with the exact per-op kernels (a
+  // later part may have read the unproven part's outputs).  Must be called
+  // before anything reads the segment's outputs or popcounts or launches
+  // work that depends on them; a no-op when nothing is pending.
+  void resolve();
+  bool pending() const;
 
   void set_schedule(const Schedule& s);
   // True when every kernel `run` would launch for this segment is already

@@ -138,6 +138,15 @@ int bsz_bind_input(bsz_run* run, const char* name, int64_t index, const uint64_t
 int bsz_bind_broadcast(bsz_run* run, const char* name, const uint8_t* ones, int64_t count);
 /* Runs the program.  stats may be NULL. */
 int bsz_execute(bsz_run* run, bsz_stats* stats);
+/* Asynchronous form of bsz_execute: walks the program and enqueues its device
+   work on the context's stream, then returns without waiting (no host
+   read-back), so the host can prepare the next run while the device works.
+   bsz_run_wait waits, checks the fused kernels' speculation (re-running
+   unproven parts exactly), reads the popcounts and fills `stats` (may be
+   NULL).  Reading a result of a launched run waits implicitly.  A run's
+   inputs must stay unchanged until it has finished. */
+int bsz_execute_async(bsz_run* run);
+int bsz_run_wait(bsz_run* run, bsz_stats* stats);
 /* Results.  For a stream output: copies ceil(bitlength/64) words (bits at and
  * above the bitlength cleared, as the reference masks outputs) into host
  * memory.  index < 0 for scalar outputs.  Returns nonzero if absent. */
