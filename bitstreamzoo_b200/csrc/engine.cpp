@@ -526,6 +526,7 @@ bool Executor::nonzero(int node, const Stmt* at) {
   int x = node;
   auto it = at ? live_->at.find(at->id) : live_->at.end();
   flush(it == live_->at.end() ? nullptr : &it->second, &x);
+  if (fused_) fused_->resolve();   // the condition reads the segment's output
   BSZ_CUDA(cudaMemsetAsync(d_flag_, 0, 4, dev_.stream()));
   launch_any(dev_, nodes_[x].buf->p, nw_, d_flag_);
   unsigned int h = 0;
