@@ -454,16 +454,21 @@ def measure_workload(E, workload: str, nbits: int, steps: int, warmup: int, main
                      "(median of 3 device-timed runs each, before the timed region)")
         # what the shipped cost model would have picked with no timing, from
         # the same sweep (no extra runs)
+        names = [k for k, _ in bz._lib.Schedule._fields_]
+        short = ("warps", "min_blocks", "prefetch", "cut_adds", "layout", "chunk_words", "stages", "ctas_per_sm")
+        sweep_top = [{"schedule": {k: v for k, v in zip(names, key) if k in short}, "ms": round(ms, 4)}
+                     for key, ms in sorted(times.items(), key=lambda kv: kv[1])[:6]]
+        model_pick = {"sweep_fastest": sweep_top}
         model = tuner.CostModel.load_default(ctx)
         if model is not None:
             best_ms = min(times.values())
             m1 = model.choose(prog, nbits)
             ranked = model.rank(tuner.program_features(prog), nbits, tuner.CANDIDATES)
-            model_pick = {"top1_schedule": m1, "top1_ms": times[tuner.schedule_key(m1)],
+            model_pick.update({"top1_schedule": m1, "top1_ms": times[tuner.schedule_key(m1)],
                           "tuned_ms": best_ms, "top1_regret": times[tuner.schedule_key(m1)] / best_ms - 1,
                           "top4_regret": min(times[tuner.schedule_key(s)] for s in ranked[:4]) / best_ms - 1,
                           "default_regret": times[tuner.schedule_key(dict(bz.DEFAULT_SCHEDULE))] / best_ms - 1
-                          if tuner.schedule_key(dict(bz.DEFAULT_SCHEDULE)) in times else None}
+                          if tuner.schedule_key(dict(bz.DEFAULT_SCHEDULE)) in times else None})
     elif schedule in ("model", "model1"):
         from bitstreamzoo_b200 import tuner
         model = tuner.CostModel.load_default(ctx)
@@ -657,7 +662,7 @@ def measure_workload(E, workload: str, nbits: int, steps: int, warmup: int, main
         "ms_per_step": main.get("ms", float("nan")) / steps, "steps": steps, "warmup": warmup,
         "data": W.data,
         "config": {"workload": W.desc + " (per GPU)", "form": main_mode, "bits_per_stream": nbits,
-                   "schedule": sched, "schedule_source": sched_src, "cost_model_pick": model_pick,
+                   "schedule": sched, "schedule_source": sched_src, "sweep": model_pick,
                    "l2": ("inputs larger than L2; no flush needed" if W.in_bytes > (126 << 20)
                           else "inputs fit in L2 (reported, not roofline-judged)"),
                    "parallelism": f"replicas x{world} (independent stream sets)"},
