@@ -34,12 +34,35 @@ Device::~Device() {
   if (d_scan_) cudaFree(d_scan_);
   if (d_err_) cudaFree(d_err_);
   if (d_scratch_) cudaFree(d_scratch_);
+  for (auto& kv : *pinned_free_) cudaFreeHost(kv.second);
+  pinned_free_->clear();
   for (int k = 0; k < 2; ++k) {
     if (pin_[k]) cudaFreeHost(pin_[k]);
     if (pin_ev_[k]) cudaEventDestroy(pin_ev_[k]);
     if (exec_ev_[k]) cudaEventDestroy(exec_ev_[k]);
   }
   if (stream_) cudaStreamDestroy(stream_);
+}
+
+std::shared_ptr<void> Device::pinned_block(size_t bytes) {
+  bytes = std::max<size_t>(4096, (bytes + 4095) / 4096 * 4096);
+  void* p = nullptr;
+  size_t have = bytes;
+  auto it = pinned_free_->lower_bound(bytes);
+  if (it != pinned_free_->end() && it->first <= 4 * bytes) {
+    have = it->first;
+    p = it->second;
+    pinned_free_->erase(it);
+  } else {
+    BSZ_CUDA(cudaHostAlloc(&p, bytes, cudaHostAllocDefault));
+  }
+  // the cache outlives the Device only through blocks still referenced:
+  // those are freed directly when the Device is gone
+  std::weak_ptr<std::multimap<size_t, void*>> pool = pinned_free_;
+  return std::shared_ptr<void>(p, [pool, have](void* q) {
+    if (auto m = pool.lock()) m->emplace(have, q);
+    else cudaFreeHost(q);
+  });
 }
 
 namespace {

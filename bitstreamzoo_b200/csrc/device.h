@@ -92,6 +92,11 @@ class Device {
   // Untyped device scratch (cached; grows).
   void* scratch(size_t bytes);
 
+  // A pinned host block of at least `bytes` for asynchronous read-backs,
+  // from a cache (cudaHostAlloc only when none fits); it returns to the
+  // cache when the last reference goes.
+  std::shared_ptr<void> pinned_block(size_t bytes);
+
   // Copies between pageable host memory and the device through two pinned
   // staging buffers: chunks are double-buffered (the host memcpy of one
   // chunk, split across threads, overlaps the DMA of the other), so large
@@ -121,6 +126,7 @@ class Device {
   void* d_scratch_ = nullptr;
   size_t scratch_cap_ = 0;
   void* pin_[2] = {nullptr, nullptr};
+  std::shared_ptr<std::multimap<size_t, void*>> pinned_free_ = std::make_shared<std::multimap<size_t, void*>>();
   cudaEvent_t pin_ev_[2] = {nullptr, nullptr};
   cudaEvent_t exec_ev_[2] = {nullptr, nullptr};
   void ensure_pinned();

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <cstring>
 #include <cstdlib>
 #include <functional>
 
@@ -212,7 +213,12 @@ Executor::~Executor() {
                  walk_replayed ? 1 : 0, t_segment_ms, t_policy_ms, t_run_ms,
                  fused_ ? fused_->t_prelaunch_ms : 0.0, fused_ ? fused_->t_wait_ms : 0.0, t_compact_ms,
                  compile_ms);
-  cudaStreamSynchronize(dev_.stream());
+  // A finished run's device work is complete.  Otherwise wait for it before
+  // its buffers go back to the device's cache (reuse is stream-ordered, but a
+  // caller may free a borrowed input as soon as the run is gone).  Waiting
+  // after finish() would also wait for whatever another run enqueued since.
+  if (!finished_) cudaStreamSynchronize(dev_.stream());
+  if (done_ev_) cudaEventDestroy(done_ev_);
   // flag, slot and VM buffers go back to the device's cache with their BufRefs
 }
 
@@ -650,12 +656,52 @@ void Executor::run(bool finish_now) {
       for (auto& kv : arrs_[id]->elems) materialize(kv.second);
   }
   if (finish_now) finish();
+  else enqueue_readback();
+}
+
+void Executor::enqueue_readback() {
+  rb_slots_ = n_slots_ - resolved_upto_;
+  rb_flags_ = fused_ ? fused_->pending_parts() : 0;
+  readback_ = dev_.pinned_block(static_cast<size_t>(8 * rb_slots_ + 4 * rb_flags_ + 8));
+  char* h = static_cast<char*>(readback_.get());
+  if (rb_slots_ > 0)
+    BSZ_CUDA(cudaMemcpyAsync(h, d_slots_ + (resolved_upto_ - slot_base_), static_cast<size_t>(rb_slots_) * 8,
+                             cudaMemcpyDeviceToHost, dev_.stream()));
+  if (rb_flags_ > 0) fused_->enqueue_flags(reinterpret_cast<uint32_t*>(h + 8 * rb_slots_));
+  BSZ_CUDA(cudaMemcpyAsync(h + 8 * rb_slots_ + 4 * rb_flags_, dev_.error_word(), 4, cudaMemcpyDeviceToHost,
+                           dev_.stream()));
+  if (!done_ev_) BSZ_CUDA(cudaEventCreateWithFlags(&done_ev_, cudaEventDisableTiming));
+  BSZ_CUDA(cudaEventRecord(done_ev_, dev_.stream()));
 }
 
 void Executor::finish() {
+  if (finished_) return;
+  if (readback_) {
+    // wait for this run's work and read-backs only
+    BSZ_CUDA(cudaEventSynchronize(done_ev_));
+    const char* h = static_cast<const char*>(readback_.get());
+    uint32_t err = 0;
+    std::memcpy(&err, h + 8 * rb_slots_ + 4 * rb_flags_, 4);
+    const bool reran = rb_flags_ > 0 && fused_->resolve_with(reinterpret_cast<const uint32_t*>(h + 8 * rb_slots_));
+    if (!reran && rb_slots_ > 0) {
+      std::memcpy(slot_val_.data() + resolved_upto_, h, static_cast<size_t>(rb_slots_) * 8);
+      resolved_upto_ += rb_slots_;
+    }
+    readback_.reset();
+    if (err) {
+      BSZ_CUDA(cudaMemsetAsync(dev_.error_word(), 0, 4, dev_.stream()));
+      throw RuntimeError(describe_device_error(err));
+    }
+    if (!reran) {
+      finished_ = true;
+      return;
+    }
+    // a re-run rewrote popcount slots: read them again below (synchronously)
+  }
   if (fused_) fused_->resolve();
   resolve_slots();
   if (uint32_t err = dev_.take_error()) throw RuntimeError(describe_device_error(err));
+  finished_ = true;
 }
 
 // ----------------------------------------------------------------- flush ---

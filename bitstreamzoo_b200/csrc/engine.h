@@ -210,6 +210,15 @@ class Executor {
   struct ExecCache;
   std::string bind_sig_;
   int64_t n_flushes_ = 0;
+  bool finished_ = false;         // finish() completed: no device work of this run outstanding
+  // Asynchronous run: the read-backs (popcount slots, fused speculation
+  // flags, device error word) enqueued behind the run's work into a pinned
+  // block, and an event after them; finish() waits on that event only, not
+  // on whatever other runs enqueued since.
+  std::shared_ptr<void> readback_;
+  cudaEvent_t done_ev_ = nullptr;
+  int64_t rb_slots_ = 0, rb_flags_ = 0;
+  void enqueue_readback();
   ExecCache& exec_cache() const;
   std::string walk_key() const;
   bool replay_walk(const std::string& key);

@@ -2002,15 +2002,30 @@ void rerun_part_exact(Device& dev, const Part& p, std::unordered_map<int, Node>&
 
 void FusedBackend::resolve() {
   if (!impl_->pending) return;
-  std::unique_ptr<PendingSegment> pend = std::move(impl_->pending);
   Device& dev = impl_->dev;
-  const std::vector<Part>& parts = *pend->parts;
   using clk = std::chrono::steady_clock;
   auto tw = clk::now();
-  std::vector<uint32_t> flags(parts.size(), 0);
+  std::vector<uint32_t> flags(impl_->pending->parts->size(), 0);
   BSZ_CUDA(cudaMemcpyAsync(flags.data(), impl_->d_fail, 4 * flags.size(), cudaMemcpyDeviceToHost, dev.stream()));
   BSZ_CUDA(cudaStreamSynchronize(dev.stream()));
   t_wait_ms += std::chrono::duration<double, std::milli>(clk::now() - tw).count();
+  resolve_with(flags.data());
+}
+
+int64_t FusedBackend::pending_parts() const {
+  return impl_->pending ? static_cast<int64_t>(impl_->pending->parts->size()) : 0;
+}
+
+void FusedBackend::enqueue_flags(uint32_t* host) {
+  if (!impl_->pending) return;
+  BSZ_CUDA(cudaMemcpyAsync(host, impl_->d_fail, 4 * impl_->pending->parts->size(), cudaMemcpyDeviceToHost,
+                           impl_->dev.stream()));
+}
+
+bool FusedBackend::resolve_with(const uint32_t* flags) {
+  if (!impl_->pending) return false;
+  std::unique_ptr<PendingSegment> pend = std::move(impl_->pending);
+  const std::vector<Part>& parts = *pend->parts;
   size_t first = parts.size();
   for (size_t i = 0; i < parts.size(); ++i)
     if (flags[i]) {
@@ -2021,9 +2036,10 @@ void FusedBackend::resolve() {
   // every later part (which may have read its outputs), with the plain
   // per-op kernels (exact by construction).
   for (size_t i = first; i < parts.size(); ++i) {
-    rerun_part_exact(dev, parts[i], pend->nodes, pend->N, pend->nw, pend->d_slots);
+    rerun_part_exact(impl_->dev, parts[i], pend->nodes, pend->N, pend->nw, pend->d_slots);
     if (flags[i]) ++fallbacks;
   }
+  return first < parts.size();
 }
 
 // ================================================================ batches ==

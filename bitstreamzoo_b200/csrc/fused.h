@@ -30,6 +30,13 @@ class FusedBackend {
   // work that depends on them; a no-op when nothing is pending.
   void resolve();
   bool pending() const;
+  // Asynchronous form of resolve(): enqueue_flags copies the pending
+  // segment's flags (pending_parts() words) to pinned host memory on the
+  // stream; once that copy has completed, resolve_with(flags) re-runs what
+  // is unproven and returns true if it re-ran anything.
+  int64_t pending_parts() const;
+  void enqueue_flags(uint32_t* host);
+  bool resolve_with(const uint32_t* flags);
 
   void set_schedule(const Schedule& s);
   // True when every kernel `run` would launch for this segment is already
