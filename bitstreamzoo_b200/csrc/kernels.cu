@@ -209,8 +209,8 @@ k_shr(uint64_t* __restrict__ d, const uint64_t* __restrict__ a, int64_t ws, int 
 // into lane i = bit i of ((G|P)+G+cin) ^ P, carry out = bit 32.  Across
 // steps the (g, p) pairs compose.
 constexpr int kAddWarps = 8;   // warps per CTA (independent tiles)
-constexpr int kAddSteps = 16;
-constexpr int kAddMinBlocks = 1;
+constexpr int kAddSteps = 8;   // 256-word tiles; 16-step tiles need ~150 registers (one CTA per SM)
+constexpr int kAddMinBlocks = 2;
 constexpr int64_t kAddTile = kAddSteps * 32;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;

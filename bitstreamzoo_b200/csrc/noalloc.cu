@@ -7,10 +7,10 @@
 // allocator, or a latency-critical loop that cannot afford the implicit
 // device-wide synchronisation of cudaMalloc/cudaFree.  For them this file
 // provides bsz_add_noalloc(): the same single-pass carry-scan addition as
-// bsz_op_add(), but its look-back scratch (one status word per 512-word
+// bsz_op_add(), but its look-back scratch (one status word per 256-word
 // tile, a tile ticket and an error word) lives in a fixed-size file-scope
 // __device__ array instead of memory from cudaMalloc.  Every GPU that loads
-// the library's device code holds this array (about 513 KiB) until the
+// the library's device code holds this array (about 1 MiB) until the
 // process exits.  The CUDA runtime loads that code on a device lazily, at the
 // first kernel launch or symbol lookup there, and that load commits the
 // array: it is the one device allocation this entry point causes, and it
@@ -36,8 +36,8 @@ namespace {
 // Largest stream: 2^26 words = 2^32 bits (512 MiB per operand).
 constexpr int64_t kMaxWords = int64_t(1) << 26;
 // Look-back state for kMaxWords: one ticket word + one status word per tile
-// of 512 words (checked against the kernel's own sizing at set-up).
-constexpr int64_t kStateWords = 1 + kMaxWords / 512;
+// of 256 words (checked against the kernel's own sizing at set-up).
+constexpr int64_t kStateWords = 1 + kMaxWords / 256;
 // The error word sits after the state, on its own 256-byte line.
 constexpr int64_t kErrOffset = ((kStateWords + 63) / 64) * 64;
 constexpr int64_t kScratchWords = kErrOffset + 64;

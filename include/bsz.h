@@ -263,11 +263,11 @@ int bsz_s2p(bsz_ctx* ctx, const uint8_t* bytes, int64_t n_bytes, uint64_t* const
  * of cudaMalloc/cudaFree.  Same result as bsz_op_add (dst = a + b with bits
  * at and above `bitlength` cleared; the same bitlength and in-place rules);
  * no context is needed.  The look-back scratch is a fixed file-scope device
- * array of about 513 KiB, so n_words is limited to 2^26 (streams of up to
+ * array of about 1 MiB, so n_words is limited to 2^26 (streams of up to
  * 2^32 bits); longer streams are rejected with an error.  The CUDA runtime
  * loads the library's device code on a device lazily, and that load commits
  * the array, which the device then keeps until the process exits: the first
- * call on each device therefore allocates those 513 KiB once.  Callers that
+ * call on each device therefore allocates that 1 MiB once.  Callers that
  * must never allocate later make one set-up call per device at start-up,
  * while allocation is still allowed and before any stream capture; a call
  * with n_words = 0 does only that set-up (pointers unused).  Every call
