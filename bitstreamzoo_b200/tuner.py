@@ -399,8 +399,9 @@ def tuning_suite(n_train: int = 24, n_test: int = 8, seed: int = 20261210, max_o
     Each DAG draws its op mix from Dirichlet(1) over five classes (AND/OR/
     XOR, shift left, ADD, shift right, NOT), its size log-uniformly from 50
     to ``max_ops`` generator ops, an operand window from {all, 6, 24, 96}
-    and a maximum shift distance from {1, 7, 70}.  The held-out set ends
-    with the 300- and 2,000-op regex-shaped DAGs."""
+    and a maximum shift distance from {1, 7, 70}.  The held-out set starts
+    with the 300- and 2,000-op regex-shaped DAGs (so a time-budgeted study
+    always evaluates them)."""
     from .workloads import regex_dag_src, shaped_dag_src
 
     rng = np.random.default_rng(seed)
@@ -413,8 +414,8 @@ def tuning_suite(n_train: int = 24, n_test: int = 8, seed: int = 20261210, max_o
                               max_shift=int(rng.choice([1, 7, 70])))
 
     train = [draw(k) for k in range(n_train)]
-    test = [draw(1000 + k) for k in range(max(0, n_test - 2))]
-    test += [regex_dag_src(n_ops=300, seed=seed + 7), regex_dag_src(n_ops=2000)][: max(0, n_test)]
+    test = [regex_dag_src(n_ops=300, seed=seed + 7), regex_dag_src(n_ops=2000)][: max(0, n_test)]
+    test += [draw(1000 + k) for k in range(max(0, n_test - 2))]
     return train, test
 
 
@@ -503,7 +504,8 @@ def precompile(srcs, candidates=None, nbits: int = 1 << 22, threads: int | None 
 
 def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candidates=None,
           sample_frac: float = 0.5, reps: int = 3, steps: int = 1500, seed: int = 0, log=None,
-          weight_decay: float = 0.05, precompile_threads: int = 0) -> dict:
+          weight_decay: float = 0.05, precompile_threads: int = 0, train_budget_s: float | None = None,
+          test_budget_s: float | None = None, batch: int = 24) -> dict:
     """Collects timings, fits a :class:`CostModel` and reports pick regret on
     the held-out programs for the model's top-1 and top-4 picks and for the
     default schedule.
@@ -512,7 +514,10 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candida
     it, so each training program draws a ``sample_frac`` share of the
     code-generation variants (warps, register cap, prefetch, add cuts) and
     times every launch variant of those at every length.  Held-out programs
-    are timed exhaustively (that is the regret's reference)."""
+    are timed exhaustively (that is the regret's reference).  Programs are
+    compiled and timed in batches of ``batch``; with ``train_budget_s`` /
+    ``test_budget_s`` no new batch starts once that many seconds of the phase
+    have passed (the report gives how many programs each phase used)."""
     import time as _time
 
     candidates = candidates or CANDIDATES
@@ -535,13 +540,21 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candida
     for i in range(len(train_srcs)):
         k = max(1, int(round(sample_frac * len(variants))))
         chosen_by.append({variants[j] for j in rng.choice(len(variants), size=k, replace=False)})
-    if precompile_threads:
-        t_pc = precompile(train_srcs + test_srcs, candidates, threads=precompile_threads, log=log,
-                          only=chosen_by + [None] * len(test_srcs))
-        if log:
-            log(f"precompiled in {t_pc:.0f}s")
+    t_pc = 0.0
+
+    def compile_batch(srcs, only):
+        nonlocal t_pc
+        if precompile_threads:
+            t_pc += precompile(srcs, candidates, threads=precompile_threads, only=only)
+
     t0 = _time.time()
+    n_train_used = len(train_srcs)
     for i, src in enumerate(train_srcs):
+        if i % batch == 0:
+            if train_budget_s is not None and _time.time() - t0 > train_budget_s:
+                n_train_used = i
+                break
+            compile_batch(train_srcs[i:i + batch], chosen_by[i:i + batch])
         prog, pf = prog_of(src)
         chosen = chosen_by[i]
         for n in sizes:
@@ -564,7 +577,14 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candida
     default_key = schedule_key(DEFAULT_SCHEDULE)
     rows = []
     raw_test = []
+    t2 = _time.time()
+    n_test_used = len(test_srcs)
     for i, src in enumerate(test_srcs):
+        if i % batch == 0:
+            if test_budget_s is not None and _time.time() - t2 > test_budget_s:
+                n_test_used = i
+                break
+            compile_batch(test_srcs[i:i + batch], None)
         prog, pf = prog_of(src)
         for n in sizes:
             times = {schedule_key(s): measure(ctx, prog, n, bufs_by_size[n][1], s, reps=reps)
@@ -595,8 +615,9 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candida
         v = np.array([r[key] for r in rows])
         return {"mean": float(v.mean()), "median": float(np.median(v)), "max": float(v.max())}
 
-    return {"model": model, "rows": rows, "n_candidates": len(candidates), "n_train_programs": len(train_srcs),
-            "n_test_programs": len(test_srcs), "sizes": list(sizes), "sample_frac": sample_frac,
+    return {"model": model, "rows": rows, "n_candidates": len(candidates), "n_train_programs": n_train_used,
+            "n_test_programs": n_test_used, "sizes": list(sizes), "sample_frac": sample_frac,
+            "precompile_s": t_pc, "test_s": _time.time() - t2,
             "n_train_timings": n_timed, "loss_first": float(np.mean(losses[:20])),
             "loss_last": float(np.mean(losses[-20:])), "collect_s": t_collect, "fit_s": t_fit,
             "regret_top1": stats("regret_top1"), "regret_top4": stats("regret_top4"),
@@ -627,11 +648,17 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=1500)
     ap.add_argument("--max-ops", type=int, default=3000)
     ap.add_argument("--threads", type=int, default=16, help="parallel precompile threads (0: none)")
+    ap.add_argument("--sizes", default="22,25,28", help="log2 stream lengths (bits), comma-separated")
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--train-budget", type=float, default=None, help="seconds: no new training batch after")
+    ap.add_argument("--test-budget", type=float, default=None, help="seconds: no new held-out batch after")
     a = ap.parse_args(argv)
     ctx = Context(0)
     train, test = tuning_suite(a.train, a.test, max_ops=a.max_ops)
-    rep = study(ctx, train, test, sample_frac=a.sample_frac, steps=a.steps,
-                log=lambda m: print(m, flush=True), precompile_threads=a.threads)
+    sizes = tuple(1 << int(x) for x in a.sizes.split(","))
+    rep = study(ctx, train, test, sizes=sizes, sample_frac=a.sample_frac, steps=a.steps, reps=a.reps,
+                log=lambda m: print(m, flush=True), precompile_threads=a.threads,
+                train_budget_s=a.train_budget, test_budget_s=a.test_budget)
     model = rep.pop("model")
     if a.out:
         model.save(a.out)
