@@ -48,7 +48,7 @@ struct bsz_run {
   std::vector<std::pair<int, int64_t>> params;
   bool launched = false;   // bsz_execute_async enqueued its work
   bool done = false;       // finished: results readable
-  int64_t l0 = 0;          // the device's launch count before this run
+  int64_t l0 = 0, l1 = 0;  // the device's launch count before and after this run's launches
   cudaEvent_t ev[2] = {nullptr, nullptr};   // device-time window of this run
   ~bsz_run() {
     ex.reset();
@@ -295,6 +295,7 @@ static void launch_run(bsz_run* run) {
   BSZ_CUDA(cudaEventRecord(run->ev[0], dev.stream()));
   ex.run(false);
   BSZ_CUDA(cudaEventRecord(run->ev[1], dev.stream()));
+  run->l1 = dev.n_launches;   // other runs may launch before this one is waited on
   run->launched = true;
 }
 
@@ -303,7 +304,9 @@ static void finish_run(bsz_run* run, bsz_stats* stats) {
   bsz::Device& dev = *run->prog->ctx->dev;
   bsz::Executor& ex = executor(run);
   if (!run->done) {
-    ex.finish();
+    const int64_t f0 = dev.n_launches;
+    ex.finish();   // may re-run unproven fused parts
+    run->l1 += dev.n_launches - f0;
     BSZ_CUDA(cudaEventSynchronize(run->ev[1]));
     run->done = true;
   }
@@ -311,7 +314,7 @@ static void finish_run(bsz_run* run, bsz_stats* stats) {
     float ms = 0;
     cudaEventElapsedTime(&ms, run->ev[0], run->ev[1]);
     stats->op_count = ex.op_count;
-    stats->n_kernel_launches = dev.n_launches - run->l0;
+    stats->n_kernel_launches = run->l1 - run->l0;
     stats->n_mallocs = dev.n_mallocs;
     stats->n_segments = ex.n_segments;
     stats->n_syncs = ex.n_syncs;

@@ -183,7 +183,8 @@ def test_async_runs_overlap_and_stay_exact(ctx):
             assert np.array_equal(r.stream("r"), want_r), sched
             assert r.int("n") == want_n, sched
     # a run that needs no re-run, read without an explicit wait
-    src2 = "input stream a\ninput stream b\noutput stream c\noutput int m\nc = (a + b) ^ (a << 3)\nm = popcount(c)\n"
+    src2 = ("input stream a\ninput stream b\noutput stream c\noutput int m\n"
+            "stream s = a + b\nstream t = a << 3\nc = s ^ t\nm = popcount(c)\n")
     ins2 = {"a": wl.random_words(rng, nbits), "b": wl.random_words(rng, nbits)}
     p2 = ctx.compile(src2)
     want = ctx.run(p2, nbits, ins2, mode=bz.MODE_PLAIN)
