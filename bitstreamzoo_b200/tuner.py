@@ -515,9 +515,9 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candida
     code-generation variants (warps, register cap, prefetch, add cuts) and
     times every launch variant of those at every length.  Held-out programs
     are timed exhaustively (that is the regret's reference).  Programs are
-    compiled and timed in batches of ``batch``; with ``train_budget_s`` /
-    ``test_budget_s`` no new batch starts once that many seconds of the phase
-    have passed (the report gives how many programs each phase used)."""
+    compiled in batches of ``batch``; with ``train_budget_s`` /
+    ``test_budget_s`` no new program starts once that many seconds of the
+    phase have passed (the report gives how many programs each phase used)."""
     import time as _time
 
     candidates = candidates or CANDIDATES
@@ -550,10 +550,10 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candida
     t0 = _time.time()
     n_train_used = len(train_srcs)
     for i, src in enumerate(train_srcs):
+        if train_budget_s is not None and _time.time() - t0 > train_budget_s:
+            n_train_used = i
+            break
         if i % batch == 0:
-            if train_budget_s is not None and _time.time() - t0 > train_budget_s:
-                n_train_used = i
-                break
             compile_batch(train_srcs[i:i + batch], chosen_by[i:i + batch])
         prog, pf = prog_of(src)
         chosen = chosen_by[i]
@@ -580,10 +580,10 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candida
     t2 = _time.time()
     n_test_used = len(test_srcs)
     for i, src in enumerate(test_srcs):
+        if test_budget_s is not None and _time.time() - t2 > test_budget_s:
+            n_test_used = i
+            break
         if i % batch == 0:
-            if test_budget_s is not None and _time.time() - t2 > test_budget_s:
-                n_test_used = i
-                break
             compile_batch(test_srcs[i:i + batch], None)
         prog, pf = prog_of(src)
         for n in sizes:
