@@ -43,6 +43,7 @@
 #include <set>
 #include <sstream>
 #include <unordered_map>
+#include <unordered_set>
 
 namespace bsz {
 namespace {
@@ -1689,7 +1690,19 @@ struct PendingSegment {
   std::unordered_map<int, Node> nodes;
   int64_t N = 0, nw = 0;
   unsigned long long* d_slots = nullptr;
+  std::string spec_key;   // non-empty: the segment ran with speculative carries (scheme 0)
 };
+
+// Segments (graph and schedule keys) whose speculative carry state could not
+// be proven once: whether it can depends on how the DAG correlates the
+// operands of its additions, so the next run of the same segment would most
+// likely fail again and pay for the exact re-run.  Such a segment runs its
+// additions with the look-back carry scan (carry scheme 2) from then on.
+std::mutex g_spec_mu;
+std::unordered_set<std::string>& spec_failed() {
+  static std::unordered_set<std::string> s;
+  return s;
+}
 
 struct FusedBackend::Impl {
   Device& dev;
@@ -1781,7 +1794,21 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
   using clk = std::chrono::steady_clock;
   auto ms_since = [](clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); };
   auto tp = clk::now();
-  const std::string skey = graph_key(nodes, seg.order, seg.inputs, seg.outputs, seg.pops, (N % 64) != 0, sc);
+  std::string skey = graph_key(nodes, seg.order, seg.inputs, seg.outputs, seg.pops, (N % 64) != 0, sc);
+  std::string spec_key;
+  if (sc.cut_adds == 0) {
+    bool failed_before;
+    {
+      std::lock_guard<std::mutex> lk(g_spec_mu);
+      failed_before = spec_failed().count(skey) != 0;
+    }
+    if (failed_before) {
+      sc.cut_adds = 2;
+      skey = graph_key(nodes, seg.order, seg.inputs, seg.outputs, seg.pops, (N % 64) != 0, sc);
+    } else {
+      spec_key = skey;
+    }
+  }
   std::shared_ptr<const SegPlan> plan;
   {
     std::lock_guard<std::mutex> lk(g_plan_mu);
@@ -1941,6 +1968,7 @@ void FusedBackend::run(std::vector<Node>& nodes, const Segment& seg, int64_t N, 
   pend->N = N;
   pend->nw = nw;
   pend->d_slots = d_slots;
+  pend->spec_key = std::move(spec_key);
   for (const Part& p : plan->parts) {
     for (int n : p.order) pend->nodes.emplace(n, nodes[n]);
     for (int n : p.inputs) pend->nodes.emplace(n, nodes[n]);
@@ -2038,6 +2066,11 @@ bool FusedBackend::resolve_with(const uint32_t* flags) {
   for (size_t i = first; i < parts.size(); ++i) {
     rerun_part_exact(impl_->dev, parts[i], pend->nodes, pend->N, pend->nw, pend->d_slots);
     if (flags[i]) ++fallbacks;
+  }
+  if (first < parts.size() && !pend->spec_key.empty()) {
+    std::lock_guard<std::mutex> lk(g_spec_mu);
+    if (spec_failed().size() >= kMaxPlans) spec_failed().clear();
+    spec_failed().insert(pend->spec_key);
   }
   return first < parts.size();
 }

@@ -32,7 +32,8 @@ FORMS = [(bz.MODE_PLAIN, None), (bz.MODE_FUSED, {"layout": 0}), (bz.MODE_FUSED, 
          (bz.MODE_FUSED, {"layout": 1, "warps": 4, "min_blocks": 1, "shift_mul": 1}),
          (bz.MODE_FUSED, {"layout": 1, "chunk_words": 8, "warps": 4, "min_blocks": 1}),
          (bz.MODE_FUSED, {"layout": 1, "warps": 4, "min_blocks": 1, "cut_adds": 2}),
-         (bz.MODE_FUSED, {"layout": 0, "cut_adds": 2})]
+         (bz.MODE_FUSED, {"layout": 0, "cut_adds": 2}),
+         (bz.MODE_FUSED, {"layout": 2, "chunk_words": 4, "warps": 8, "min_blocks": 1, "cut_adds": 2})]
 
 
 def run_both(ctx, src, nbits, inputs):
@@ -195,3 +196,24 @@ def test_async_runs_overlap_and_stay_exact(ctx):
         r.launch()
     assert r2.int("m") == want.int("m")
     assert np.array_equal(r1.stream("c"), want.stream("c"))
+
+
+@pytest.mark.gpu
+def test_segment_whose_speculation_failed_switches_to_lookback_adds(ctx):
+    """After a segment's speculative carry state could not be proven once,
+    the next run of the same segment and schedule takes its additions through
+    the look-back carry scan: no re-run, the same exact result."""
+    nbits = (1 << 21) + 9
+    rng = np.random.default_rng(12)
+    src = ("input stream x\ninput stream z\noutput stream r\noutput int n\n"
+           "stream y = ~x\nstream s = x + y\nstream t = s << 3\nr = t + z\nn = popcount(r)\n")
+    inputs = {"x": wl.random_words(rng, nbits), "z": wl.random_words(rng, nbits)}
+    want = ctx.run(src, nbits, inputs, mode=bz.MODE_PLAIN)
+    sched = {"layout": 1, "warps": 8, "min_blocks": 1}
+    first = ctx.run(src, nbits, inputs, mode=bz.MODE_FUSED, schedule=sched)
+    second = ctx.run(src, nbits, inputs, mode=bz.MODE_FUSED, schedule=sched)
+    assert first.stats["n_fused_fallbacks"] >= 1
+    assert second.stats["n_fused_fallbacks"] == 0
+    for r in (first, second):
+        assert np.array_equal(r.stream("r"), want.stream("r"))
+        assert r.int("n") == want.int("n")
