@@ -64,7 +64,7 @@ def parse_args():
     ap.add_argument("--no-extra", action="store_true",
                     help="default run: skip the regex_dag and batched workloads (extra keys of the line)")
     ap.add_argument("--schedule", default="tuned", choices=["tuned", "model", "model1", "default"],
-                    help="fused-kernel schedule: the autotuner's pick (every candidate of the 16-schedule "
+                    help="fused-kernel schedule: the autotuner's pick (every candidate of the 32-schedule "
                          "space timed before the timed region), the fastest of the shipped cost model's 4 "
                          "best predictions, the model's top-1 pick (no timing), or the default")
     ap.add_argument("--schedule-json", default=None,
