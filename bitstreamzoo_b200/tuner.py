@@ -262,6 +262,11 @@ class CostModel:
         self.sd = np.ones(in_dim, np.float32)
         self.y_mu = 0.0
         self.y_sd = 1.0
+        # the training rows' feature range: inputs are clipped to it, so a
+        # program or length outside the training suite (longer streams, more
+        # outputs) is predicted as the nearest trained one, not extrapolated
+        self.lo = None
+        self.hi = None
 
     def __del__(self):
         try:
@@ -329,6 +334,7 @@ class CostModel:
                 y[sel] -= y[sel].mean()
         self.mu = X.mean(0)
         self.sd = np.maximum(X.std(0), 1e-3).astype(np.float32)
+        self.lo, self.hi = X.min(0), X.max(0)
         self.y_mu = float(y.mean())
         self.y_sd = float(max(y.std(), 1e-3))
         Xs = (X - self.mu) / self.sd
@@ -344,7 +350,10 @@ class CostModel:
         return losses
 
     def predict_ms(self, X) -> np.ndarray:
-        X = (np.asarray(X, np.float32) - self.mu) / self.sd
+        X = np.asarray(X, np.float32)
+        if self.lo is not None:
+            X = np.clip(X, self.lo, self.hi)
+        X = (X - self.mu) / self.sd
         return np.exp(self.raw_predict(X).astype(np.float64) * self.y_sd + self.y_mu)
 
     def rank(self, pfeat: list[float], nbits: int, candidates=None) -> list[dict]:
@@ -364,8 +373,9 @@ class CostModel:
         return ranked[min(timed)[1]]
 
     def save(self, path: str):
+        extra = {} if self.lo is None else {"lo": self.lo, "hi": self.hi}
         np.savez(path, params=self.params(), mu=self.mu, sd=self.sd, y=np.array([self.y_mu, self.y_sd]),
-                 in_dim=np.array([self.in_dim]))
+                 in_dim=np.array([self.in_dim]), **extra)
 
     @classmethod
     def load_default(cls, ctx, path: str | None = None):
@@ -388,6 +398,8 @@ class CostModel:
         self.set_params(z["params"])
         self.mu, self.sd = z["mu"], z["sd"]
         self.y_mu, self.y_sd = float(z["y"][0]), float(z["y"][1])
+        if "lo" in z:
+            self.lo, self.hi = z["lo"], z["hi"]
 
 
 # ------------------------------------------------------------------- study --
