@@ -517,7 +517,7 @@ def precompile(srcs, candidates=None, nbits: int = 1 << 22, threads: int | None 
 def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candidates=None,
           sample_frac: float = 0.5, reps: int = 3, steps: int = 1500, seed: int = 0, log=None,
           weight_decay: float = 0.05, precompile_threads: int = 0, train_budget_s: float | None = None,
-          test_budget_s: float | None = None, batch: int = 24) -> dict:
+          test_budget_s: float | None = None, batch: int = 24, collect_only: bool = False) -> dict:
     """Collects timings, fits a :class:`CostModel` and reports pick regret on
     the held-out programs for the model's top-1 and top-4 picks and for the
     default schedule.
@@ -529,7 +529,8 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candida
     are timed exhaustively (that is the regret's reference).  Programs are
     compiled in batches of ``batch``; with ``train_budget_s`` /
     ``test_budget_s`` no new program starts once that many seconds of the
-    phase have passed (the report gives how many programs each phase used)."""
+    phase have passed (the report gives how many programs each phase used).
+    ``collect_only`` returns the training rows without fitting."""
     import time as _time
 
     candidates = candidates or CANDIDATES
@@ -581,6 +582,9 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candida
         if log:
             log(f"train {i + 1}/{len(train_srcs)} timed={n_timed} t={_time.time() - t0:.0f}s")
     t_collect = _time.time() - t0
+    if collect_only:
+        return {"X": X, "y": y, "groups": groups, "n_train_programs": n_train_used, "n_train_timings": n_timed,
+                "precompile_s": t_pc, "collect_s": t_collect}
     model = CostModel(ctx, len(X[0]), seed=seed + 1, weight_decay=weight_decay)
     t1 = _time.time()
     losses = model.fit(X, y, steps=steps, seed=seed, groups=groups)
@@ -642,6 +646,41 @@ def study(ctx, train_srcs, test_srcs, sizes=(1 << 22, 1 << 25, 1 << 28), candida
             "raw": {"train_X": X, "train_ms": y, "train_groups": groups, "test": raw_test}}
 
 
+def extend(ctx, prev: dict, train_srcs, sizes, steps: int = 1500, seed: int = 0, weight_decay: float = 0.05,
+           **collect) -> tuple:
+    """Adds training rows at new lengths to a previous study's report
+    (``prev``, with its ``raw`` timings), refits on all rows and re-scores
+    the previous held-out cases from their recorded timings (no re-timing).
+    Returns (model, summary)."""
+    new = study(ctx, train_srcs, [], sizes=sizes, seed=seed, collect_only=True, **collect)
+    raw = prev["raw"]
+    X = list(raw["train_X"]) + new["X"]
+    y = list(raw["train_ms"]) + new["y"]
+    # new groups: offset past every (program, length) id of the previous rows
+    groups = list(raw["train_groups"]) + [10 ** 6 + g for g in new["groups"]]
+    model = CostModel(ctx, len(X[0]), seed=seed + 1, weight_decay=weight_decay)
+    losses = model.fit(X, y, steps=steps, seed=seed, groups=groups)
+    rows = []
+    for c in raw["test"]:
+        ms = np.asarray(c["ms"], np.float64)
+        order = np.argsort(model.predict_ms(c["X"]), kind="stable")
+        best = float(ms.min())
+        rows.append({"regret_top1": ms[order[0]] / best - 1, "regret_top4": ms[order[:4]].min() / best - 1,
+                     "regret_default": c["default_ms"] / best - 1, "regret_random": float(ms.mean()) / best - 1})
+
+    def stats(key):
+        v = np.array([r[key] for r in rows])
+        return {"mean": float(v.mean()), "median": float(np.median(v)), "max": float(v.max())}
+
+    summary = {"n_rows": len(X), "n_new_rows": len(new["X"]), "n_new_programs": new["n_train_programs"],
+               "new_sizes": list(sizes), "collect_s": new["collect_s"], "precompile_s": new["precompile_s"],
+               "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-20:])),
+               "held_out_cases": len(rows)}
+    for k in ("regret_top1", "regret_top4", "regret_default", "regret_random"):
+        summary[k] = stats(k)
+    return model, summary
+
+
 def main(argv=None):
     """python -m bitstreamzoo_b200.tuner [--out model.npz] [--json report.json]
     runs :func:`study` on the default suite and saves the fitted model."""
@@ -664,10 +703,26 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--train-budget", type=float, default=None, help="seconds: no new training batch after")
     ap.add_argument("--test-budget", type=float, default=None, help="seconds: no new held-out batch after")
+    ap.add_argument("--extend", default=None,
+                    help="a previous study's JSON report: time its first --train training programs at --sizes, "
+                         "refit on all rows, re-score its held-out cases")
     a = ap.parse_args(argv)
     ctx = Context(0)
     train, test = tuning_suite(a.train, a.test, max_ops=a.max_ops)
     sizes = tuple(1 << int(x) for x in a.sizes.split(","))
+    if a.extend:
+        with open(a.extend) as f:
+            prev = json.load(f)
+        model, summary = extend(ctx, prev, train, sizes, steps=a.steps, sample_frac=a.sample_frac, reps=a.reps,
+                                log=lambda m: print(m, flush=True), precompile_threads=a.threads,
+                                train_budget_s=a.train_budget)
+        if a.out:
+            model.save(a.out)
+        print(json.dumps(summary))
+        if a.json:
+            with open(a.json, "w") as f:
+                json.dump(summary, f, indent=1)
+        return 0
     rep = study(ctx, train, test, sizes=sizes, sample_frac=a.sample_frac, steps=a.steps, reps=a.reps,
                 log=lambda m: print(m, flush=True), precompile_threads=a.threads,
                 train_budget_s=a.train_budget, test_budget_s=a.test_budget)
