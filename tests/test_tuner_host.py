@@ -36,6 +36,19 @@ def test_schedule_encoding():
     assert len(e) == tuner.N_SCHEDULE_FEATURES
     assert e[0] == 2.0 and e[4] == 1.0 and e[5] == 0.0
     assert e[6] == math.log2(32 * 4 * 4)
+    # warp form: no thread-form knobs, speculative carries
+    assert e[7:] == [0.0, 0.0, 0.0, 0.0, 0.0, 0.0]
+    # register form with 8-word chunks and look-back additions
+    r = tuner.encode_schedule(dict(DEFAULT_SCHEDULE, layout=1, chunk_words=8, cut_adds=2, min_blocks=1))
+    assert r[5] == 0.0 and r[7] == 1.0 and r[8] == 0.0 and r[9] == 3.0 and r[12] == 1.0
+    # TMA form, 3 stages, materialized additions
+    t = tuner.encode_schedule(dict(DEFAULT_SCHEDULE, layout=2, stages=3, cut_adds=1))
+    assert t[5] == 1.0 and t[7] == 1.0 and t[8] == 1.0 and t[9] == 2.0 and t[10] == 3.0 and t[12] == 0.0
+
+
+def test_every_candidate_has_a_distinct_encoding():
+    rows = {tuple(tuner.encode_schedule(s)) for s in tuner.CANDIDATES}
+    assert len(rows) == len(tuner.CANDIDATES)
 
 
 def test_regret():
