@@ -664,7 +664,7 @@ def measure_workload(E, workload: str, nbits: int, steps: int, warmup: int, main
         "config": {"workload": W.desc + " (per GPU)", "form": main_mode, "bits_per_stream": nbits,
                    "schedule": sched, "schedule_source": sched_src, "sweep": model_pick,
                    "l2": ("inputs larger than L2; no flush needed" if W.in_bytes > (126 << 20)
-                          else "inputs fit in L2 (reported, not roofline-judged)"),
+                          else "inputs fit in L2 (reported, not held to the HBM roofline)"),
                    "parallelism": f"replicas x{world} (independent stream sets)"},
         "hbm_frac_step": main.get("hbm_frac_step"), "roofline": roof, "cpu_baseline": cb, "e2e": e2e,
         "gpu_launches": main.get("launches"), "clocks": main.get("clocks"), "check": check,
