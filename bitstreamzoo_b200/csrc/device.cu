@@ -39,7 +39,6 @@ Device::~Device() {
   for (int k = 0; k < 2; ++k) {
     if (pin_[k]) cudaFreeHost(pin_[k]);
     if (pin_ev_[k]) cudaEventDestroy(pin_ev_[k]);
-    if (exec_ev_[k]) cudaEventDestroy(exec_ev_[k]);
   }
   if (stream_) cudaStreamDestroy(stream_);
 }
@@ -91,11 +90,6 @@ void parallel_memcpy(void* dst, const void* src, size_t n) {
 }
 
 }  // namespace
-
-cudaEvent_t Device::exec_event(int i) {
-  if (!exec_ev_[i]) BSZ_CUDA(cudaEventCreate(&exec_ev_[i]));
-  return exec_ev_[i];
-}
 
 void Device::ensure_pinned() {
   if (pin_[0]) return;

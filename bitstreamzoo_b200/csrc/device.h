@@ -86,8 +86,6 @@ class Device {
   int64_t bytes_live = 0;
   int64_t bytes_peak = 0;
 
-  // Two timing events reused by every execution on this device.
-  cudaEvent_t exec_event(int i);
 
   // Untyped device scratch (cached; grows).
   void* scratch(size_t bytes);
@@ -128,7 +126,6 @@ class Device {
   void* pin_[2] = {nullptr, nullptr};
   std::shared_ptr<std::multimap<size_t, void*>> pinned_free_ = std::make_shared<std::multimap<size_t, void*>>();
   cudaEvent_t pin_ev_[2] = {nullptr, nullptr};
-  cudaEvent_t exec_ev_[2] = {nullptr, nullptr};
   void ensure_pinned();
   void* raw_alloc(size_t bytes);
   struct ProfRec { const char* name; cudaEvent_t a, b; };
